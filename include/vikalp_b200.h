@@ -1,0 +1,186 @@
+/*
+ * vikalp_b200.h -- C ABI of the B200 (sm_100a) PDHG LP / PDQP library.
+ *
+ * This is the boundary VIKALP's CUDA route binds to. It replaces, for LP and
+ * convex QP, the reference's CUDA ExecutionBackend
+ * (include/vikalp/backend/CudaBackend.hpp:18-20, cuda/cuda_ops.cu) plus the
+ * backend-driven PDHG / PDQP loops that run on it
+ * (src/solver/lp/pdhg.cpp:20-265, src/solver/qp/pdqp.cpp:20-298). The C++
+ * router (vikalp::solve, include/vikalp/solver/Solver.hpp) calls these entry
+ * points when SolverOptions::backend == BackendPreference::CUDA.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only; all matrices are CSR with int64 offsets
+ *     and indices and float64 values, exactly the reference's CsrPattern /
+ *     CsrMatrix (include/vikalp/contracts/Model.hpp:16-26).
+ *   - Every function returns VK_OK (0) or a negative status; nothing throws
+ *     across the ABI. vk_last_error() gives the message of the calling
+ *     thread's most recent failure.
+ *   - Host pointers unless the name says _device. Device pointers are
+ *     addresses on the current CUDA device.
+ *   - A handle is owned by one thread at a time and owns one CUDA stream
+ *     ("create one backend per thread", CudaBackend.hpp:17).
+ */
+#ifndef VIKALP_B200_H
+#define VIKALP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define VK_OK 0
+#define VK_ERR_INVALID (-1)     /* invalid input: SolveStatus::InvalidModel      */
+#define VK_ERR_UNSUPPORTED (-2) /* unsupported model/method: UnsupportedModel     */
+#define VK_ERR_CUDA (-3)        /* CUDA runtime failure: NumericalFailure         */
+#define VK_ERR_INTERNAL (-4)    /* any other failure: NumericalFailure            */
+
+/* SolveStatus values (include/vikalp/contracts/SolveResult.hpp:11-24). */
+enum {
+    VK_STATUS_NOT_SOLVED = 0,
+    VK_STATUS_OPTIMAL = 1,
+    VK_STATUS_ITERATION_LIMIT = 6,
+    VK_STATUS_TIME_LIMIT = 8,
+    VK_STATUS_NUMERICAL_FAILURE = 9,
+    VK_STATUS_UNSUPPORTED_MODEL = 10,
+    VK_STATUS_INVALID_MODEL = 11
+};
+
+/* Iteration schemes. */
+enum {
+    /* The reference's restarted PDHG / PDQP, iterate for iterate
+     * (pdhg.cpp:87-151, pdqp.cpp:110-178): single-pass infinity-norm scaling,
+     * tau = sigma, step halving / growth every 50 iterations, absolute
+     * infinity-norm stop in scaled coordinates. */
+    VK_ALGO_REFERENCE = 0,
+    /* Restarted reflected-Halpern PDHG: Ruiz + Pock-Chambolle scaling, power
+     * iteration step size, primal weight, fixed-point-residual restarts and a
+     * relative-KKT stop in original coordinates. */
+    VK_ALGO_HALPERN = 1
+};
+
+enum { VK_PREC_FP64 = 0, VK_PREC_MIXED = 1 };
+
+/* Sparse products: FAST uses warp-cooperative sums for long rows;
+ * SEQUENTIAL sums every row left to right in CSR order, which is the order the
+ * reference's CPU backend uses (cpu_ops.cpp:418-427, 444-458), so results
+ * are bit-identical to it. */
+enum { VK_SPMV_FAST = 0, VK_SPMV_SEQUENTIAL = 1 };
+
+typedef struct {
+    int64_t rows, cols;
+    const int64_t *row_offsets; /* [rows + 1], row_offsets[0] == 0 */
+    const int64_t *col_indices; /* [nnz], strictly increasing per row */
+    const double *values;       /* [nnz] */
+} vk_csr;
+
+/* Canonical model (Model.hpp:38-44): min c'x + 0.5 x'Qx + offset
+ * s.t. row_lower <= A x <= row_upper, var_lower <= x <= var_upper. */
+typedef struct {
+    vk_csr A;        /* m x n */
+    vk_csr Q;        /* n x n full symmetric CSR, or rows == cols == 0 for an LP */
+    const double *c; /* [n] */
+    double objective_offset;
+    const double *var_lower, *var_upper; /* [n], -inf / +inf allowed */
+    const double *row_lower, *row_upper; /* [m], -inf / +inf allowed */
+} vk_problem;
+
+/* Mirrors vikalp::SolverOptions (SolverOptions.hpp:15-28) plus the B200
+ * extensions. Fill with vk_default_options() first. */
+typedef struct {
+    int64_t iteration_limit;   /* SolverOptions::iteration_limit (100000)       */
+    double time_limit_seconds; /* SolverOptions::time_limit_seconds (+inf)      */
+    double primal_tolerance;   /* SolverOptions::primal_tolerance (1e-7)        */
+    double dual_tolerance;     /* SolverOptions::dual_tolerance (1e-7)          */
+    int32_t continuous_method; /* SolverOptions::continuous_method: 0 Auto,     */
+                               /* 1 PDHG, 2 RevisedSimplex, 3 InteriorPoint (0) */
+    int32_t algorithm;         /* VK_ALGO_*                    (REFERENCE)      */
+    int32_t precision;         /* VK_PREC_*                    (FP64)           */
+    int32_t spmv_order;        /* VK_SPMV_*                    (FAST)           */
+    int32_t check_every;       /* iterations per device-side check (64)         */
+    double relative_tolerance; /* HALPERN stop: relative KKT (1e-6)             */
+    int32_t device;            /* CUDA device ordinal (0)                       */
+    int32_t verbose;           /* 0: silent                                      */
+} vk_options;
+
+/* Outputs. Array pointers are caller-allocated host buffers or NULL. */
+typedef struct {
+    double *x;              /* [n] primal solution, original coordinates      */
+    double *y;              /* [m] row multipliers (y > 0: upper row active)   */
+    double *row_lower_dual; /* [m] SolveResult::constraint_lower_dual          */
+    double *row_upper_dual; /* [m] SolveResult::constraint_upper_dual          */
+    double *var_lower_dual; /* [n] SolveResult::variable_lower_dual            */
+    double *var_upper_dual; /* [n] SolveResult::variable_upper_dual            */
+    int32_t status;         /* VK_STATUS_*                                      */
+    int64_t iterations;
+    int64_t restarts;
+    double objective;
+    double primal_residual, stationarity_residual, complementarity_residual;
+    double rel_primal, rel_dual, rel_gap; /* relative KKT of the returned point  */
+    double last_metric;                   /* the reference's scaled max(inf-norms) */
+    double solve_seconds;
+    double iterate_seconds; /* device time of the iteration loop alone */
+    int64_t fp32_iterations; /* MIXED: iterations done in FP32 */
+    char message[256];
+} vk_result;
+
+typedef struct vk_pdhg vk_pdhg;
+
+void vk_default_options(vk_options *opts);
+const char *vk_last_error(void);
+const char *vk_version(void);
+
+/* Validates the model as Model::validate + solve_lp/solve_qp do
+ * (Model.cpp:118-199, continuous_common.hpp:80-126), copies it to the GPU and
+ * builds every device-side structure (int32 CSR, transposed CSR, scaling,
+ * tile schedules). Replaces the setup half of solve_scaled_lp / qp
+ * (pdhg.cpp:20-80, pdqp.cpp:20-103). */
+int vk_pdhg_create(const vk_problem *problem, const vk_options *opts, vk_pdhg **out);
+
+/* Runs the solve. warm_start, var_lower_override and var_upper_override are
+ * NULL or n long (RelaxationOracle.hpp:15-16, continuous_common.hpp:80-110).
+ * Replaces the loop and post-processing of solve_scaled_lp / qp
+ * (pdhg.cpp:87-264, pdqp.cpp:110-297). Model errors (bad overrides, a
+ * non-finite warm start) return VK_OK with result->status INVALID_MODEL, as the
+ * reference returns a SolveResult rather than throwing. */
+int vk_pdhg_solve(vk_pdhg *h, const double *warm_start, const double *var_lower_override,
+                  const double *var_upper_override, vk_result *result);
+
+void vk_pdhg_destroy(vk_pdhg *h);
+
+/* ---- primitives (ExecutionBackend-level, ExecutionBackend.hpp:36-64) ------ */
+
+/* CSR transpose on the GPU by a stable counting sort on the column index, so
+ * that rows ascend within each column (the accumulation order of the
+ * reference's transposed product, cpu_ops.cpp:449-458). Host arrays:
+ * t_row_offsets[cols+1], t_col_indices[nnz] (= source rows), t_values[nnz]
+ * (may be NULL), perm[nnz] (source position of each entry; may be NULL). */
+int vk_csr_transpose(const vk_csr *a, int64_t *t_row_offsets, int64_t *t_col_indices,
+                     double *t_values, int64_t *perm);
+
+/* y = alpha * op(A) * x + beta * y with host arrays
+ * (ExecutionBackend::multiply, cpu_ops.cpp:393-460 / cuda_ops.cu:473-528).
+ * transpose != 0 computes A' * x through a transposed CSR built on the GPU. */
+int vk_spmv(const vk_csr *a, double alpha, const double *x, double beta, double *y, int transpose,
+            int spmv_order);
+
+/* A reusable sparse operator resident on the GPU, for repeated products on
+ * device vectors (the bench's SpMV bandwidth figure uses it). */
+typedef struct vk_spmat vk_spmat;
+/* precision: VK_PREC_FP64 stores float64 values, VK_PREC_MIXED float32. */
+int vk_spmat_create(const vk_csr *a, int32_t precision, vk_spmat **out);
+/* y = A x (transpose == 0) or A' x (transpose != 0) on device arrays of the
+ * matrix's precision, on `stream` (a cudaStream_t, NULL = default stream). */
+int vk_spmat_apply_device(vk_spmat *m, const void *x_device, void *y_device, int transpose,
+                          void *stream);
+/* Algorithmic bytes one vk_spmat_apply_device call moves (values, int32
+ * indices, int32 offsets, x once, y once). */
+int64_t vk_spmat_bytes(const vk_spmat *m, int transpose);
+void vk_spmat_destroy(vk_spmat *m);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VIKALP_B200_H */

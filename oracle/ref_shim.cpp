@@ -1,0 +1,267 @@
+// C-ABI shim over the reference VIKALP CPU path -- TEST / BASELINE INFRASTRUCTURE ONLY.
+//
+// oracle/Makefile compiles this file together with the reference's own
+// sources (read in place from the reference tree, never copied) into
+// oracle/_ref/libvkref.so. It lets the tests pin the C oracle against the real
+// reference and lets bench.py time the reference's CPU implementation.
+//
+// Entry points:
+//   vkref_solve_lp / vkref_solve_qp -> vikalp::solver::solve_lp / solve_qp with
+//                                      make_cpu_backend() (continuous.hpp:10-22)
+//   vkref_solve                     -> vikalp::solve(Model, SolverOptions) (Solver.hpp:19-21)
+//   vkref_multiply                  -> ExecutionBackend::multiply on the CPU backend
+//                                      (cpu_ops.cpp:393-460)
+//   vkref_pdhg_replay               -> the per-iteration ExecutionBackend call sequence of
+//                                      pdhg.cpp:92-130 on already-scaled data, for sizes where
+//                                      the reference's own setup cannot finish (its column
+//                                      scaling is O(n*nnz), continuous_common.hpp:160-176).
+#include "vikalp/backend/CpuBackend.hpp"
+#include "vikalp/contracts/ExecutionBackend.hpp"
+#include "vikalp/contracts/Model.hpp"
+#include "vikalp/contracts/SolveResult.hpp"
+#include "vikalp/contracts/SolverOptions.hpp"
+#include "vikalp/solver/Solver.hpp"
+#include "vikalp/solver/continuous.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <limits>
+#include <span>
+#include <string>
+#include <vector>
+
+extern "C" {
+
+typedef struct {
+    int64_t m, n;
+    const int64_t *ro, *ci;
+    const double *v;
+    int64_t q_nnz;
+    const int64_t *qro, *qci;
+    const double *qv;
+    const double *c, *rl, *ru;
+    double objective_offset;
+    const double *l, *u;
+} vkref_problem;
+
+typedef struct {
+    int64_t iteration_limit;
+    double time_limit_seconds;
+    double primal_tolerance, dual_tolerance;
+    int32_t backend; // BackendPreference
+    int32_t method;  // ContinuousMethod
+} vkref_options;
+
+typedef struct {
+    double *x, *row_lower_dual, *row_upper_dual, *var_lower_dual, *var_upper_dual; // caller-allocated or NULL
+    int32_t status;
+    int64_t iterations;
+    double objective, primal_residual, stationarity_residual, complementarity_residual;
+    double dual_bound, solve_seconds;
+    char solver[32];
+    char backend[32];
+    char message[256];
+} vkref_result;
+}
+
+namespace {
+
+vikalp::Model build_model(const vkref_problem *p) {
+    vikalp::Model model;
+    model.name = "vkref";
+    const auto m = static_cast<std::size_t>(p->m), n = static_cast<std::size_t>(p->n);
+    const auto nnz = static_cast<std::size_t>(p->ro[p->m]);
+    model.linear_objective.assign(p->c, p->c + n);
+    model.objective_offset = p->objective_offset;
+    model.variable_lower.assign(p->l, p->l + n);
+    model.variable_upper.assign(p->u, p->u + n);
+    model.variable_types.assign(n, vikalp::VariableType::Continuous);
+    model.constraint_lower.assign(p->rl, p->rl + m);
+    model.constraint_upper.assign(p->ru, p->ru + m);
+    model.constraint_matrix.pattern.rows = p->m;
+    model.constraint_matrix.pattern.columns = p->n;
+    model.constraint_matrix.pattern.row_offsets.assign(p->ro, p->ro + m + 1);
+    model.constraint_matrix.pattern.column_indices.assign(p->ci, p->ci + nnz);
+    model.constraint_matrix.values.assign(p->v, p->v + nnz);
+    if (p->q_nnz > 0) {
+        model.quadratic_objective.pattern.rows = p->n;
+        model.quadratic_objective.pattern.columns = p->n;
+        model.quadratic_objective.pattern.row_offsets.assign(p->qro, p->qro + n + 1);
+        model.quadratic_objective.pattern.column_indices.assign(p->qci, p->qci + p->q_nnz);
+        model.quadratic_objective.values.assign(p->qv, p->qv + p->q_nnz);
+    }
+    return model;
+}
+
+vikalp::SolverOptions build_options(const vkref_options *o) {
+    vikalp::SolverOptions opts;
+    opts.iteration_limit = o->iteration_limit;
+    opts.time_limit_seconds = o->time_limit_seconds;
+    opts.primal_tolerance = o->primal_tolerance;
+    opts.dual_tolerance = o->dual_tolerance;
+    opts.backend = static_cast<vikalp::BackendPreference>(o->backend);
+    opts.continuous_method = static_cast<vikalp::ContinuousMethod>(o->method);
+    return opts;
+}
+
+void copy_out(const std::vector<double> &src, double *dst) {
+    if (dst && !src.empty()) std::memcpy(dst, src.data(), src.size() * sizeof(double));
+}
+
+void fill_result(const vikalp::SolveResult &r, vkref_result *out) {
+    out->status = static_cast<int32_t>(r.status);
+    out->iterations = r.iterations;
+    out->objective = r.objective_value;
+    out->primal_residual = r.primal_residual;
+    out->stationarity_residual = r.stationarity_residual;
+    out->complementarity_residual = r.complementarity_residual;
+    out->dual_bound = r.dual_bound;
+    out->solve_seconds = r.solve_seconds;
+    copy_out(r.primal_solution, out->x);
+    copy_out(r.constraint_lower_dual, out->row_lower_dual);
+    copy_out(r.constraint_upper_dual, out->row_upper_dual);
+    copy_out(r.variable_lower_dual, out->var_lower_dual);
+    copy_out(r.variable_upper_dual, out->var_upper_dual);
+    std::snprintf(out->solver, sizeof(out->solver), "%s", r.solver.c_str());
+    std::snprintf(out->backend, sizeof(out->backend), "%s", r.backend.c_str());
+    std::snprintf(out->message, sizeof(out->message), "%s", r.message.c_str());
+}
+
+std::span<const double> opt_span(const double *p, int64_t n) {
+    return p ? std::span<const double>(p, static_cast<std::size_t>(n)) : std::span<const double>{};
+}
+
+} // namespace
+
+extern "C" {
+
+int vkref_solve_continuous(const vkref_problem *p, const vkref_options *o, const double *warm,
+                           const double *lo, const double *hi, int qp, vkref_result *out) {
+    try {
+        const auto model = build_model(p);
+        auto backend = vikalp::make_cpu_backend();
+        const auto opts = build_options(o);
+        const auto r = qp ? vikalp::solver::solve_qp(model, *backend, opts, opt_span(warm, p->n),
+                                                     opt_span(lo, p->n), opt_span(hi, p->n))
+                          : vikalp::solver::solve_lp(model, *backend, opts, opt_span(warm, p->n),
+                                                     opt_span(lo, p->n), opt_span(hi, p->n));
+        fill_result(r, out);
+        return 0;
+    } catch (const std::exception &e) {
+        std::snprintf(out->message, sizeof(out->message), "%s", e.what());
+        return -1;
+    }
+}
+
+int vkref_solve(const vkref_problem *p, const vkref_options *o, vkref_result *out) {
+    try {
+        const auto model = build_model(p);
+        const auto r = vikalp::solve(model, build_options(o));
+        fill_result(r, out);
+        return 0;
+    } catch (const std::exception &e) {
+        std::snprintf(out->message, sizeof(out->message), "%s", e.what());
+        return -1;
+    }
+}
+
+// y = alpha * op(A) * x + beta * y on the reference CPU backend. Returns 0, or
+// -1 when the backend throws (dimension errors throw std::invalid_argument).
+int vkref_multiply(int64_t m, int64_t n, const int64_t *ro, const int64_t *ci, const double *v,
+                   double alpha, const double *x, int64_t x_len, double beta, double *y,
+                   int64_t y_len, int transpose, char *err, int err_len) {
+    try {
+        auto be = vikalp::make_cpu_backend();
+        vikalp::CsrPattern pat;
+        pat.rows = m;
+        pat.columns = n;
+        pat.row_offsets.assign(ro, ro + m + 1);
+        pat.column_indices.assign(ci, ci + ro[m]);
+        auto mat = be->create_matrix(pat);
+        be->set_values(std::span<const double>(v, static_cast<std::size_t>(ro[m])), *mat);
+        auto xv = be->create_vector(x_len);
+        auto yv = be->create_vector(y_len);
+        be->upload(std::span<const double>(x, static_cast<std::size_t>(x_len)), *xv);
+        be->upload(std::span<const double>(y, static_cast<std::size_t>(y_len)), *yv);
+        be->multiply(alpha, *mat, *xv, beta, *yv,
+                     transpose ? vikalp::Transpose::Yes : vikalp::Transpose::No);
+        be->download(*yv, std::span<double>(y, static_cast<std::size_t>(y_len)));
+        return 0;
+    } catch (const std::exception &e) {
+        if (err && err_len > 0) std::snprintf(err, static_cast<std::size_t>(err_len), "%s", e.what());
+        return -1;
+    }
+}
+
+// Runs `iterations` passes of the pdhg.cpp:92-130 backend-call sequence (fixed
+// tau = sigma = step) on already-scaled data with the reference CPU backend.
+// Returns seconds spent in the loop; x[n] and y[m] hold the final iterates.
+double vkref_pdhg_replay(const vkref_problem *p, double step, int64_t iterations, double *x_out,
+                         double *y_out) {
+    using vikalp::Transpose;
+    auto be = vikalp::make_cpu_backend();
+    const int64_t m = p->m, n = p->n;
+    vikalp::CsrPattern pat;
+    pat.rows = m;
+    pat.columns = n;
+    pat.row_offsets.assign(p->ro, p->ro + m + 1);
+    pat.column_indices.assign(p->ci, p->ci + p->ro[m]);
+    auto A = be->create_matrix(pat);
+    be->set_values(std::span<const double>(p->v, static_cast<std::size_t>(p->ro[m])), *A);
+    auto vec = [&](int64_t k) { return be->create_vector(k); };
+    auto x = vec(n), xn = vec(n), xb = vec(n), aty = vec(n), g = vec(n), px = vec(n), res = vec(n);
+    auto c = vec(n), l = vec(n), u = vec(n);
+    auto y = vec(m), axb = vec(m), ya = vec(m), yp = vec(m), ax = vec(m), pax = vec(m), rl = vec(m), ru = vec(m);
+    be->upload(std::span<const double>(p->c, static_cast<std::size_t>(n)), *c);
+    be->upload(std::span<const double>(p->l, static_cast<std::size_t>(n)), *l);
+    be->upload(std::span<const double>(p->u, static_cast<std::size_t>(n)), *u);
+    be->upload(std::span<const double>(p->rl, static_cast<std::size_t>(m)), *rl);
+    be->upload(std::span<const double>(p->ru, static_cast<std::size_t>(m)), *ru);
+    be->fill(*x, 0.0);
+    be->project_box(*x, *l, *u);
+    be->fill(*y, 0.0);
+    const double tau = step, sigma = step;
+    double sink = 0.0;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int64_t it = 0; it < iterations; ++it) {
+        be->multiply(1.0, *A, *y, 0.0, *aty, Transpose::Yes);
+        be->copy(*x, *xn);
+        be->axpby(-tau, *c, 1.0, *xn);
+        be->axpby(-tau, *aty, 1.0, *xn);
+        be->project_box(*xn, *l, *u);
+        be->copy(*x, *xb);
+        be->axpby(2.0, *xn, -1.0, *xb);
+        be->multiply(1.0, *A, *xb, 0.0, *axb, Transpose::No);
+        be->copy(*y, *ya);
+        be->axpby(sigma, *axb, 1.0, *ya);
+        be->copy(*ya, *yp);
+        be->axpby(1.0 / sigma, *yp, 0.0, *yp);
+        be->project_box(*yp, *rl, *ru);
+        be->copy(*ya, *y);
+        be->axpby(-sigma, *yp, 1.0, *y);
+        be->copy(*xn, *x);
+        be->multiply(1.0, *A, *x, 0.0, *ax, Transpose::No);
+        be->copy(*ax, *pax);
+        be->project_box(*pax, *rl, *ru);
+        be->axpby(1.0, *pax, -1.0, *ax);
+        sink += be->norm_inf(*ax);
+        be->multiply(1.0, *A, *y, 0.0, *aty, Transpose::Yes);
+        be->copy(*c, *g);
+        be->axpby(1.0, *aty, 1.0, *g);
+        be->copy(*x, *px);
+        be->axpby(-1.0, *g, 1.0, *px);
+        be->project_box(*px, *l, *u);
+        be->copy(*x, *res);
+        be->axpby(-1.0, *px, 1.0, *res);
+        sink += be->norm_inf(*res);
+    }
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (x_out) be->download(*x, std::span<double>(x_out, static_cast<std::size_t>(n)));
+    if (y_out) be->download(*y, std::span<double>(y_out, static_cast<std::size_t>(m)));
+    return secs + 0.0 * sink;
+}
+
+} // extern "C"

@@ -1,0 +1,119 @@
+"""GPU sparse products and CSR transpose through the C ABI, against the
+reference's known answers (golden fixtures) and the CPU oracle.
+
+SEQUENTIAL order must equal the reference bit for bit; FAST order within
+1e-12 relative (sums of long rows are reassociated)."""
+
+import numpy as np
+import pytest
+
+import vikalp_b200 as vk
+from conftest import same_bits
+from vikalp_b200 import synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def _golden_spmv_names(golden):
+    return sorted({k.split("__")[0] for k in golden.files if k.startswith("spmv_")})
+
+
+@pytest.mark.parametrize("order", ["sequential", "fast"])
+def test_spmv_golden(golden, order):
+    for name in _golden_spmv_names(golden):
+        g = lambda k: golden[f"{name}__{k}"]  # noqa: E731
+        ro, n = g("ro"), int(g("n"))
+        m = len(ro) - 1
+        got = vk.spmv(ro, g("ci"), g("v"), m, n, g("x"), g("y"), float(g("alpha")), float(g("beta")),
+                      bool(int(g("transpose"))), order)
+        assert same_bits(got, g("out")), (name, got, g("out"))
+
+
+def _ragged(seed, m=700, n=900, nnz=9000):
+    inst = synthetic.lp_powerlaw(m, n, nnz, seed=seed)
+    return inst.row_offsets, inst.col_idx, inst.values, inst.m, inst.n
+
+
+def _with_long_rows(seed):
+    # rows of 1, 40, 1500 (one tile of its own), 5000 (streamed from HBM) nonzeros
+    rng = np.random.default_rng(seed)
+    n = 6000
+    lens = [1, 40, 0, 1500, 3, 5000, 7, 0, 33]
+    ro = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    ci = np.concatenate([np.sort(rng.choice(n, size=k, replace=False)) for k in lens if k > 0]).astype(np.int64)
+    v = rng.standard_normal(len(ci))
+    return ro, ci, v, len(lens), n
+
+
+@pytest.mark.parametrize("make", [_ragged, _with_long_rows])
+@pytest.mark.parametrize("transpose", [False, True])
+def test_spmv_matches_oracle(oracle, make, transpose):
+    ro, ci, v, m, n = make(3)
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal(m if transpose else n)
+    y = rng.standard_normal(n if transpose else m)
+    if transpose:
+        want = oracle.spmv_t(ro, ci, v, n, x, 0.75, 1.5, y)
+    else:
+        want = oracle.spmv(ro, ci, v, x, 0.75, 1.5, y)
+    got = vk.spmv(ro, ci, v, m, n, x, y, 0.75, 1.5, transpose, "sequential")
+    assert same_bits(got, want)
+    fast = vk.spmv(ro, ci, v, m, n, x, y, 0.75, 1.5, transpose, "fast")
+    scale = np.abs(v).max() * np.abs(x).max() * (np.diff(ro).max() + 1) + np.abs(y).max()
+    assert np.max(np.abs(fast - want)) <= 1e-13 * scale
+
+
+def test_transpose_bit_exact(oracle):
+    for make in (_ragged, _with_long_rows):
+        ro, ci, v, m, n = make(5)
+        tro, trow, tv, perm = vk.csr_transpose(ro, ci, v, m, n)
+        wro, wrow, wv, wperm = oracle.transpose(ro, ci, v, n)
+        assert np.array_equal(tro, wro)
+        assert np.array_equal(trow, wrow)
+        assert np.array_equal(perm, wperm)
+        assert same_bits(tv, wv)
+
+
+def test_transpose_edge_shapes(oracle):
+    # empty matrix, all-empty rows, a single column
+    for ro, ci, v, m, n in [
+        (np.zeros(1, np.int64), np.zeros(0, np.int64), np.zeros(0), 0, 4),
+        (np.zeros(6, np.int64), np.zeros(0, np.int64), np.zeros(0), 5, 3),
+        (np.arange(8, dtype=np.int64), np.zeros(7, np.int64), np.arange(1.0, 8.0), 7, 1),
+    ]:
+        tro, trow, tv, perm = vk.csr_transpose(ro, ci, v, m, n)
+        wro, wrow, wv, wperm = oracle.transpose(ro, ci, v, n)
+        assert np.array_equal(tro, wro) and np.array_equal(trow, wrow) and np.array_equal(perm, wperm)
+
+
+def test_spmv_invalid_pattern_raises():
+    with pytest.raises(vk.VkError) as e:
+        vk.spmv(np.array([0, 2]), np.array([1, 0]), np.ones(2), 1, 2, np.ones(2))
+    assert e.value.code == vk.VK_ERR_INVALID
+
+
+def test_spmat_device_apply(oracle):
+    torch = pytest.importorskip("torch")
+    ro, ci, v, m, n = _ragged(8, 2000, 3000, 40000)
+    A = vk.SpMat(ro, ci, v, m, n, "fp64")
+    x = torch.randn(n, dtype=torch.float64, device="cuda")
+    y = torch.zeros(m, dtype=torch.float64, device="cuda")
+    A.apply(x.data_ptr(), y.data_ptr(), False, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    want = oracle.spmv(ro, ci, v, x.cpu().numpy())
+    assert np.max(np.abs(y.cpu().numpy() - want)) <= 1e-12 * np.abs(want).max()
+    yt = torch.zeros(n, dtype=torch.float64, device="cuda")
+    xt = torch.randn(m, dtype=torch.float64, device="cuda")
+    A.apply(xt.data_ptr(), yt.data_ptr(), True, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    want_t = oracle.spmv_t(ro, ci, v, n, xt.cpu().numpy())
+    assert np.max(np.abs(yt.cpu().numpy() - want_t)) <= 1e-12 * np.abs(want_t).max()
+    B = vk.SpMat(ro, ci, v, m, n, "mixed")
+    x32 = x.float()
+    y32 = torch.zeros(m, dtype=torch.float32, device="cuda")
+    B.apply(x32.data_ptr(), y32.data_ptr(), False, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    # fp32 storage and arithmetic: relative to the row's absolute mass
+    mass = oracle.spmv(ro, ci, np.abs(v), np.abs(x.cpu().numpy()))
+    assert np.all(np.abs(y32.cpu().numpy() - want) <= 1e-5 * (mass + 1e-30))
+    assert A.bytes() == len(ci) * 12 + 4 * (m + 1) + 8 * n + 8 * m

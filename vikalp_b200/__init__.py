@@ -1,0 +1,278 @@
+"""ctypes bindings of the B200 PDHG library (include/vikalp_b200.h).
+
+The solver itself is ``libvikalp_b200.so`` (hand-written sm_100a CUDA behind a
+C ABI); this module only marshals numpy arrays across that ABI. There is no
+CPU fallback: every call goes to the CUDA library, and importing this module
+fails loudly when the library has not been built (``python -m vikalp_b200.build``).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvikalp_b200.so")
+
+VK_OK = 0
+VK_ERR_INVALID = -1
+VK_ERR_UNSUPPORTED = -2
+VK_ERR_CUDA = -3
+VK_ERR_INTERNAL = -4
+
+ALGO_REFERENCE = 0
+ALGO_HALPERN = 1
+PREC_FP64 = 0
+PREC_MIXED = 1
+SPMV_FAST = 0
+SPMV_SEQUENTIAL = 1
+
+STATUS = {0: "NotSolved", 1: "Optimal", 2: "LocallyOptimal", 3: "Feasible", 4: "Infeasible",
+          5: "Unbounded", 6: "IterationLimit", 7: "NodeLimit", 8: "TimeLimit",
+          9: "NumericalFailure", 10: "UnsupportedModel", 11: "InvalidModel"}
+
+_i64p = C.POINTER(C.c_int64)
+_f64p = C.POINTER(C.c_double)
+
+
+class VkError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+        self.msg = msg
+
+
+class Csr(C.Structure):
+    _fields_ = [("rows", C.c_int64), ("cols", C.c_int64), ("row_offsets", _i64p),
+                ("col_indices", _i64p), ("values", _f64p)]
+
+
+class Problem(C.Structure):
+    _fields_ = [("A", Csr), ("Q", Csr), ("c", _f64p), ("objective_offset", C.c_double),
+                ("var_lower", _f64p), ("var_upper", _f64p), ("row_lower", _f64p), ("row_upper", _f64p)]
+
+
+class Options(C.Structure):
+    _fields_ = [("iteration_limit", C.c_int64), ("time_limit_seconds", C.c_double),
+                ("primal_tolerance", C.c_double), ("dual_tolerance", C.c_double),
+                ("continuous_method", C.c_int32), ("algorithm", C.c_int32), ("precision", C.c_int32),
+                ("spmv_order", C.c_int32), ("check_every", C.c_int32), ("relative_tolerance", C.c_double),
+                ("device", C.c_int32), ("verbose", C.c_int32)]
+
+
+class Result(C.Structure):
+    _fields_ = [("x", _f64p), ("y", _f64p), ("row_lower_dual", _f64p), ("row_upper_dual", _f64p),
+                ("var_lower_dual", _f64p), ("var_upper_dual", _f64p), ("status", C.c_int32),
+                ("iterations", C.c_int64), ("restarts", C.c_int64), ("objective", C.c_double),
+                ("primal_residual", C.c_double), ("stationarity_residual", C.c_double),
+                ("complementarity_residual", C.c_double), ("rel_primal", C.c_double),
+                ("rel_dual", C.c_double), ("rel_gap", C.c_double), ("last_metric", C.c_double),
+                ("solve_seconds", C.c_double), ("iterate_seconds", C.c_double),
+                ("fp32_iterations", C.c_int64), ("message", C.c_char * 256)]
+
+
+# Every symbol include/vikalp_b200.h declares, with its ctypes signature.
+_SIGNATURES = {
+    "vk_default_options": (None, [C.POINTER(Options)]),
+    "vk_last_error": (C.c_char_p, []),
+    "vk_version": (C.c_char_p, []),
+    "vk_pdhg_create": (C.c_int, [C.POINTER(Problem), C.POINTER(Options), C.POINTER(C.c_void_p)]),
+    "vk_pdhg_solve": (C.c_int, [C.c_void_p, _f64p, _f64p, _f64p, C.POINTER(Result)]),
+    "vk_pdhg_destroy": (None, [C.c_void_p]),
+    "vk_csr_transpose": (C.c_int, [C.POINTER(Csr), _i64p, _i64p, _f64p, _i64p]),
+    "vk_spmv": (C.c_int, [C.POINTER(Csr), C.c_double, _f64p, C.c_double, _f64p, C.c_int, C.c_int]),
+    "vk_spmat_create": (C.c_int, [C.POINTER(Csr), C.c_int32, C.POINTER(C.c_void_p)]),
+    "vk_spmat_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "vk_spmat_bytes": (C.c_int64, [C.c_void_p, C.c_int]),
+    "vk_spmat_destroy": (None, [C.c_void_p]),
+}
+
+_lib = None
+
+
+def lib():
+    """Loads libvikalp_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m vikalp_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().vk_last_error().decode()
+
+
+def _check(rc: int):
+    if rc != VK_OK:
+        raise VkError(rc, last_error())
+
+
+def _p(a, typ=_f64p):
+    return None if a is None else a.ctypes.data_as(typ)
+
+
+class _Keep(list):
+    def f(self, a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        self.append(a)
+        return _p(a)
+
+    def i(self, a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=np.int64)
+        self.append(a)
+        return _p(a, _i64p)
+
+
+def _csr(keep: _Keep, rows, cols, ro, ci, v) -> Csr:
+    return Csr(rows, cols, keep.i(ro), keep.i(ci), keep.f(v))
+
+
+def options(**kw) -> Options:
+    o = Options()
+    lib().vk_default_options(C.byref(o))
+    names = {"algorithm": {"reference": ALGO_REFERENCE, "halpern": ALGO_HALPERN},
+             "precision": {"fp64": PREC_FP64, "mixed": PREC_MIXED},
+             "spmv_order": {"fast": SPMV_FAST, "sequential": SPMV_SEQUENTIAL}}
+    for k, v in kw.items():
+        if k in names and isinstance(v, str):
+            v = names[k][v]
+        setattr(o, k, v)
+    return o
+
+
+def problem_struct(inst, keep: _Keep) -> Problem:
+    """A vk_problem pointing into the arrays of a ``synthetic.Instance``-like object."""
+    p = Problem()
+    p.A = _csr(keep, inst.m, inst.n, inst.row_offsets, inst.col_idx, inst.values)
+    if getattr(inst, "q_col_idx", None) is not None and inst.q_nnz > 0:
+        p.Q = _csr(keep, inst.n, inst.n, inst.q_row_offsets, inst.q_col_idx, inst.q_values)
+    else:
+        p.Q = Csr(0, 0, keep.i(np.zeros(1, np.int64)), None, None)
+    p.c = keep.f(inst.c)
+    p.objective_offset = float(getattr(inst, "objective_offset", 0.0))
+    p.var_lower, p.var_upper = keep.f(inst.var_lower), keep.f(inst.var_upper)
+    p.row_lower, p.row_upper = keep.f(inst.row_lower), keep.f(inst.row_upper)
+    return p
+
+
+class Pdhg:
+    """A model resident on the GPU (vk_pdhg_create) that can be solved repeatedly."""
+
+    def __init__(self, inst, **opts):
+        self._keep = _Keep()
+        self.m, self.n = inst.m, inst.n
+        self.opts = options(**opts)
+        prob = problem_struct(inst, self._keep)
+        h = C.c_void_p()
+        _check(lib().vk_pdhg_create(C.byref(prob), C.byref(self.opts), C.byref(h)))
+        self._h = h
+        self._keep.clear()
+
+    def solve(self, warm=None, lower=None, upper=None, duals: bool = True) -> dict:
+        keep = _Keep()
+        m, n = self.m, self.n
+        out = {"x": np.zeros(n), "y": np.zeros(m)}
+        if duals:
+            out.update(row_lower_dual=np.zeros(m), row_upper_dual=np.zeros(m),
+                       var_lower_dual=np.zeros(n), var_upper_dual=np.zeros(n))
+        r = Result()
+        for k, a in out.items():
+            setattr(r, k, _p(a))
+        _check(lib().vk_pdhg_solve(self._h, keep.f(warm), keep.f(lower), keep.f(upper), C.byref(r)))
+        out.update(status=STATUS.get(r.status, str(r.status)), iterations=r.iterations, restarts=r.restarts,
+                   objective=r.objective, primal_residual=r.primal_residual,
+                   stationarity_residual=r.stationarity_residual,
+                   complementarity_residual=r.complementarity_residual, rel_primal=r.rel_primal,
+                   rel_dual=r.rel_dual, rel_gap=r.rel_gap, last_metric=r.last_metric,
+                   solve_seconds=r.solve_seconds, iterate_seconds=r.iterate_seconds,
+                   fp32_iterations=r.fp32_iterations, message=r.message.decode())
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().vk_pdhg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def solve(inst, warm=None, lower=None, upper=None, **opts) -> dict:
+    """Create + solve + destroy: the one-shot C-ABI route."""
+    with Pdhg(inst, **opts) as h:
+        return h.solve(warm, lower, upper)
+
+
+def spmv(ro, ci, v, rows, cols, x, y=None, alpha=1.0, beta=0.0, transpose=False, order="fast"):
+    keep = _Keep()
+    a = _csr(keep, rows, cols, ro, ci, v)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    ylen = cols if transpose else rows
+    y = np.zeros(ylen) if y is None else np.array(y, dtype=np.float64, copy=True)
+    _check(lib().vk_spmv(C.byref(a), alpha, _p(x), beta, _p(y), int(transpose),
+                         SPMV_SEQUENTIAL if order == "sequential" else SPMV_FAST))
+    return y
+
+
+def csr_transpose(ro, ci, v, rows, cols):
+    keep = _Keep()
+    a = _csr(keep, rows, cols, ro, ci, v)
+    nnz = int(np.asarray(ro)[rows]) if rows >= 0 else 0
+    tro = np.zeros(cols + 1, np.int64)
+    tci = np.zeros(max(nnz, 1), np.int64)
+    tv = np.zeros(max(nnz, 1))
+    perm = np.zeros(max(nnz, 1), np.int64)
+    _check(lib().vk_csr_transpose(C.byref(a), _p(tro, _i64p), _p(tci, _i64p), _p(tv), _p(perm, _i64p)))
+    return tro, tci[:nnz], tv[:nnz], perm[:nnz]
+
+
+class SpMat:
+    """A sparse operator resident on the GPU; apply() works on device pointers."""
+
+    def __init__(self, ro, ci, v, rows, cols, precision="fp64"):
+        keep = _Keep()
+        a = _csr(keep, rows, cols, ro, ci, v)
+        h = C.c_void_p()
+        _check(lib().vk_spmat_create(C.byref(a), PREC_MIXED if precision == "mixed" else PREC_FP64, C.byref(h)))
+        self._h = h
+        self.rows, self.cols = rows, cols
+
+    def apply(self, x_ptr: int, y_ptr: int, transpose: bool = False, stream: int = 0):
+        _check(lib().vk_spmat_apply_device(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), int(transpose),
+                                           C.c_void_p(stream)))
+
+    def bytes(self, transpose: bool = False) -> int:
+        return int(lib().vk_spmat_bytes(self._h, int(transpose)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().vk_spmat_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,317 @@
+// extern "C" entry points of include/vikalp_b200.h. Every call catches and
+// maps exceptions to status codes; the message is kept per thread.
+#include "vk_engine.cuh"
+
+#include <cstring>
+#include <memory>
+#include <string>
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_error(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+template <class F>
+int guarded(F &&f) {
+    try {
+        return f();
+    } catch (const vk::CudaFailure &e) {
+        return set_error(VK_ERR_CUDA, e.what());
+    } catch (const vk::InvalidInput &e) {
+        return set_error(VK_ERR_INVALID, e.what());
+    } catch (const vk::Unsupported &e) {
+        return set_error(VK_ERR_UNSUPPORTED, e.what());
+    } catch (const std::bad_alloc &) {
+        return set_error(VK_ERR_INTERNAL, "out of host memory");
+    } catch (const std::exception &e) {
+        return set_error(VK_ERR_INTERNAL, e.what());
+    } catch (...) {
+        return set_error(VK_ERR_INTERNAL, "unknown failure");
+    }
+}
+
+// CsrPattern checks of the reference backends (cpu_ops.cpp:38-63,
+// cuda_ops.cu:48-76): offsets start at 0 and ascend, columns in range and
+// strictly increasing per row.
+void check_csr(const vk_csr *a) {
+    if (!a) throw vk::InvalidInput("matrix is null");
+    if (a->rows < 0 || a->cols < 0) throw vk::InvalidInput("matrix dimensions must be non-negative");
+    if (a->rows >= (int64_t(1) << 31) || a->cols >= (int64_t(1) << 31))
+        throw vk::Unsupported("matrix exceeds the int32 index range of the device structures");
+    const int64_t *ro = a->row_offsets;
+    if (!ro) throw vk::InvalidInput("CsrPattern row_offsets size != rows+1");
+    if (ro[0] != 0) throw vk::InvalidInput("CsrPattern row_offsets do not describe column_indices");
+    const int64_t nnz = ro[a->rows];
+    if (nnz >= (int64_t(1) << 31)) throw vk::Unsupported("matrix exceeds the int32 index range");
+    for (int64_t r = 0; r < a->rows; ++r) {
+        const int64_t b = ro[r], e = ro[r + 1];
+        if (b < 0 || b > e || e > nnz) throw vk::InvalidInput("CsrPattern row_offsets must be ordered and in range");
+        int64_t prev = -1;
+        for (int64_t k = b; k < e; ++k) {
+            const int64_t c = a->col_indices[k];
+            if (c < 0 || c >= a->cols || c <= prev)
+                throw vk::InvalidInput("CsrPattern columns must be ordered and in range");
+            prev = c;
+        }
+    }
+}
+
+template <class T>
+struct PlainEpi : vk::EpiBase<T> {
+    T *y;
+    __device__ void row(int i, const T (&s)[1], double (&)[1]) const { y[i] = s[0]; }
+};
+
+// y = alpha * acc + beta * y (cpu_ops.cpp:426)
+struct AxpbyEpi : vk::EpiBase<double> {
+    double alpha, beta;
+    double *y;
+    __device__ void row(int i, const double (&s)[1], double (&)[1]) const {
+        y[i] = __dadd_rn(__dmul_rn(alpha, s[0]), __dmul_rn(beta, y[i]));
+    }
+};
+
+// y *= beta, then y[col] += v * (alpha * x[row]) in row order (cpu_ops.cpp:444-458)
+struct ScatterEpi : vk::EpiBase<double> {
+    double alpha, beta;
+    double *y;
+    __device__ double init(int j, int) const { return __dmul_rn(beta, y[j]); }
+    __device__ double gscale(int) const { return alpha; }
+    __device__ void row(int j, const double (&s)[1], double (&)[1]) const { y[j] = s[0]; }
+};
+
+struct Stream {
+    cudaStream_t s = nullptr;
+    Stream() { VK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+    ~Stream() {
+        if (s) cudaStreamDestroy(s);
+    }
+};
+
+} // namespace
+
+struct vk_pdhg {
+    std::unique_ptr<vk::Solver> solver;
+};
+
+struct vk_spmat {
+    int precision = VK_PREC_FP64;
+    vk::CsrPattern32 a, at;
+    vk::DevBuf<int> perm;
+    vk::DevBuf<double> v64, vt64;
+    vk::DevBuf<float> v32, vt32;
+};
+
+extern "C" {
+
+void vk_default_options(vk_options *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->iteration_limit = 100000;
+    o->time_limit_seconds = __builtin_inf();
+    o->primal_tolerance = 1e-7;
+    o->dual_tolerance = 1e-7;
+    o->continuous_method = 0;
+    o->algorithm = VK_ALGO_REFERENCE;
+    o->precision = VK_PREC_FP64;
+    o->spmv_order = VK_SPMV_FAST;
+    o->check_every = 64;
+    o->relative_tolerance = 1e-6;
+    o->device = 0;
+    o->verbose = 0;
+}
+
+const char *vk_last_error(void) { return g_last_error.c_str(); }
+
+const char *vk_version(void) { return "vikalp_b200 0.1 (sm_100a)"; }
+
+int vk_pdhg_create(const vk_problem *problem, const vk_options *opts, vk_pdhg **out) {
+    return guarded([&] {
+        if (!problem || !out) return set_error(VK_ERR_INVALID, "null argument");
+        *out = nullptr;
+        vk_options o;
+        if (opts)
+            o = *opts;
+        else
+            vk_default_options(&o);
+        bool unsupported = false;
+        const std::string msg = vk::validate_problem(*problem, o, unsupported);
+        if (!msg.empty()) return set_error(unsupported ? VK_ERR_UNSUPPORTED : VK_ERR_INVALID, msg);
+        auto h = std::make_unique<vk_pdhg>();
+        h->solver = std::make_unique<vk::Solver>(*problem, o);
+        *out = h.release();
+        return VK_OK;
+    });
+}
+
+int vk_pdhg_solve(vk_pdhg *h, const double *warm, const double *lo, const double *hi, vk_result *result) {
+    return guarded([&] {
+        if (!h || !result) return set_error(VK_ERR_INVALID, "null argument");
+        h->solver->solve(warm, lo, hi, result);
+        return VK_OK;
+    });
+}
+
+void vk_pdhg_destroy(vk_pdhg *h) {
+    try {
+        delete h;
+    } catch (...) {
+    }
+}
+
+int vk_csr_transpose(const vk_csr *a, int64_t *t_row_offsets, int64_t *t_col_indices, double *t_values,
+                     int64_t *perm) {
+    return guarded([&] {
+        check_csr(a);
+        Stream st;
+        vk::CsrPattern32 p, pt;
+        vk::DevBuf<int> pm;
+        static const int64_t zero = 0;
+        vk::upload_pattern(a->rows, a->cols, a->rows > 0 ? a->row_offsets : &zero, a->col_indices, p, st.s);
+        vk::transpose_pattern(p, pt, pm, st.s);
+        const int64_t nnz = p.nnz;
+        std::vector<int> tro(a->cols + 1), tci(nnz), tp(nnz);
+        VK_CUDA(cudaMemcpyAsync(tro.data(), pt.ro.get(), (a->cols + 1) * sizeof(int), cudaMemcpyDeviceToHost, st.s));
+        if (nnz > 0) {
+            VK_CUDA(cudaMemcpyAsync(tci.data(), pt.ci.get(), nnz * sizeof(int), cudaMemcpyDeviceToHost, st.s));
+            VK_CUDA(cudaMemcpyAsync(tp.data(), pm.get(), nnz * sizeof(int), cudaMemcpyDeviceToHost, st.s));
+        }
+        vk::DevBuf<double> v(nnz > 0 ? nnz : 1), tv(nnz > 0 ? nnz : 1);
+        if (t_values && nnz > 0) {
+            VK_CUDA(cudaMemcpyAsync(v.get(), a->values, nnz * sizeof(double), cudaMemcpyHostToDevice, st.s));
+            vk::gather_values<double, double>(pm.get(), v.get(), tv.get(), nnz, st.s);
+            VK_CUDA(cudaMemcpyAsync(t_values, tv.get(), nnz * sizeof(double), cudaMemcpyDeviceToHost, st.s));
+        }
+        VK_CUDA(cudaStreamSynchronize(st.s));
+        for (int64_t j = 0; j <= a->cols; ++j) t_row_offsets[j] = tro[j];
+        for (int64_t t = 0; t < nnz; ++t) t_col_indices[t] = tci[t];
+        if (perm)
+            for (int64_t t = 0; t < nnz; ++t) perm[t] = tp[t];
+        return VK_OK;
+    });
+}
+
+int vk_spmv(const vk_csr *a, double alpha, const double *x, double beta, double *y, int transpose,
+            int spmv_order) {
+    return guarded([&] {
+        check_csr(a);
+        Stream st;
+        vk::CsrPattern32 p;
+        static const int64_t zero = 0;
+        vk::upload_pattern(a->rows, a->cols, a->rows > 0 ? a->row_offsets : &zero, a->col_indices, p, st.s);
+        const int64_t nnz = p.nnz;
+        const int64_t xl = transpose ? a->rows : a->cols, yl = transpose ? a->cols : a->rows;
+        vk::DevBuf<double> v(nnz > 0 ? nnz : 1), dx(xl > 0 ? xl : 1), dy(yl > 0 ? yl : 1);
+        if (nnz > 0) VK_CUDA(cudaMemcpyAsync(v.get(), a->values, nnz * sizeof(double), cudaMemcpyHostToDevice, st.s));
+        if (xl > 0) VK_CUDA(cudaMemcpyAsync(dx.get(), x, xl * sizeof(double), cudaMemcpyHostToDevice, st.s));
+        if (yl > 0) VK_CUDA(cudaMemcpyAsync(dy.get(), y, yl * sizeof(double), cudaMemcpyHostToDevice, st.s));
+        const bool exact = spmv_order == VK_SPMV_SEQUENTIAL;
+        if (!transpose) {
+            AxpbyEpi e;
+            e.alpha = alpha;
+            e.beta = beta;
+            e.y = dy.get();
+            auto M = vk::view(p, v.get());
+            if (exact)
+                vk::launch_tiles<double, double, 1, true>(M, vk::Gathers<double, 1>{{dx.get()}}, e, st.s);
+            else
+                vk::launch_tiles<double, double, 1, false>(M, vk::Gathers<double, 1>{{dx.get()}}, e, st.s);
+        } else {
+            vk::CsrPattern32 pt;
+            vk::DevBuf<int> pm;
+            vk::transpose_pattern(p, pt, pm, st.s);
+            vk::DevBuf<double> tv(nnz > 0 ? nnz : 1);
+            vk::gather_values<double, double>(pm.get(), v.get(), tv.get(), nnz, st.s);
+            ScatterEpi e;
+            e.alpha = alpha;
+            e.beta = beta;
+            e.y = dy.get();
+            auto M = vk::view(pt, tv.get());
+            if (exact)
+                vk::launch_tiles<double, double, 1, true>(M, vk::Gathers<double, 1>{{dx.get()}}, e, st.s);
+            else
+                vk::launch_tiles<double, double, 1, false>(M, vk::Gathers<double, 1>{{dx.get()}}, e, st.s);
+        }
+        if (yl > 0) VK_CUDA(cudaMemcpyAsync(y, dy.get(), yl * sizeof(double), cudaMemcpyDeviceToHost, st.s));
+        VK_CUDA(cudaStreamSynchronize(st.s));
+        return VK_OK;
+    });
+}
+
+int vk_spmat_create(const vk_csr *a, int32_t precision, vk_spmat **out) {
+    return guarded([&] {
+        if (!out) return set_error(VK_ERR_INVALID, "null argument");
+        *out = nullptr;
+        check_csr(a);
+        if (precision != VK_PREC_FP64 && precision != VK_PREC_MIXED) return set_error(VK_ERR_INVALID, "unknown precision");
+        Stream st;
+        auto h = std::make_unique<vk_spmat>();
+        h->precision = precision;
+        static const int64_t zero = 0;
+        vk::upload_pattern(a->rows, a->cols, a->rows > 0 ? a->row_offsets : &zero, a->col_indices, h->a, st.s);
+        const int64_t nnz = h->a.nnz;
+        vk::transpose_pattern(h->a, h->at, h->perm, st.s);
+        vk::DevBuf<double> v(nnz > 0 ? nnz : 1);
+        if (nnz > 0) VK_CUDA(cudaMemcpyAsync(v.get(), a->values, nnz * sizeof(double), cudaMemcpyHostToDevice, st.s));
+        if (precision == VK_PREC_FP64) {
+            h->vt64.reset(nnz > 0 ? nnz : 1);
+            vk::gather_values<double, double>(h->perm.get(), v.get(), h->vt64.get(), nnz, st.s);
+            h->v64 = std::move(v);
+        } else {
+            h->v32.reset(nnz > 0 ? nnz : 1);
+            h->vt32.reset(nnz > 0 ? nnz : 1);
+            vk::DevBuf<int> iota;
+            // CSR order: v32[k] = v[k]
+            std::vector<int> id(nnz > 0 ? nnz : 1);
+            for (int64_t k = 0; k < nnz; ++k) id[k] = static_cast<int>(k);
+            iota.reset(id.size());
+            VK_CUDA(cudaMemcpyAsync(iota.get(), id.data(), id.size() * sizeof(int), cudaMemcpyHostToDevice, st.s));
+            vk::gather_values<float, double>(iota.get(), v.get(), h->v32.get(), nnz, st.s);
+            vk::gather_values<float, double>(h->perm.get(), v.get(), h->vt32.get(), nnz, st.s);
+            VK_CUDA(cudaStreamSynchronize(st.s));
+        }
+        VK_CUDA(cudaStreamSynchronize(st.s));
+        *out = h.release();
+        return VK_OK;
+    });
+}
+
+int vk_spmat_apply_device(vk_spmat *m, const void *x, void *y, int transpose, void *stream) {
+    return guarded([&] {
+        if (!m || !x || !y) return set_error(VK_ERR_INVALID, "null argument");
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const vk::CsrPattern32 &p = transpose ? m->at : m->a;
+        if (m->precision == VK_PREC_FP64) {
+            PlainEpi<double> e;
+            e.y = static_cast<double *>(y);
+            vk::launch_tiles<double, double, 1, false>(vk::view(p, transpose ? m->vt64.get() : m->v64.get()),
+                                                       vk::Gathers<double, 1>{{static_cast<const double *>(x)}}, e, s);
+        } else {
+            PlainEpi<float> e;
+            e.y = static_cast<float *>(y);
+            vk::launch_tiles<float, float, 1, false>(vk::view(p, transpose ? m->vt32.get() : m->v32.get()),
+                                                     vk::Gathers<float, 1>{{static_cast<const float *>(x)}}, e, s);
+        }
+        return VK_OK;
+    });
+}
+
+int64_t vk_spmat_bytes(const vk_spmat *m, int transpose) {
+    if (!m) return 0;
+    const vk::CsrPattern32 &p = transpose ? m->at : m->a;
+    const int64_t s = m->precision == VK_PREC_FP64 ? 8 : 4;
+    return p.nnz * (s + 4) + 4 * (int64_t(p.rows) + 1) + int64_t(p.cols) * s + int64_t(p.rows) * s;
+}
+
+void vk_spmat_destroy(vk_spmat *m) {
+    try {
+        delete m;
+    } catch (...) {
+    }
+}
+
+} // extern "C"

@@ -1,0 +1,196 @@
+// Device-side CSR setup: int64 -> int32 conversion, tile schedules, stable
+// transpose. All O(nnz) on the GPU.
+#include "vk_csr.cuh"
+
+#include <algorithm>
+#include <vector>
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+namespace vk {
+
+namespace {
+
+__global__ void narrow_kernel(const int64_t *__restrict__ src, int *__restrict__ dst, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = static_cast<int>(src[i]);
+}
+
+// flags[r] = 1 where a tile starts at row r (r == rows marks the end).
+__global__ void tile_flags_kernel(const int *__restrict__ ro, int rows, int *__restrict__ flags) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r > rows) return;
+    int f;
+    if (r == 0 || r == rows) {
+        f = 1;
+    } else {
+        const int a = ro[r - 1], b = ro[r], c = ro[r + 1];
+        const bool long_prev = (b - a) > kHalfTile;
+        const bool long_here = (c - b) > kHalfTile;
+        f = (long_prev || long_here || (a / kHalfTile) != (b / kHalfTile) || (r % kRowsMax) == 0) ? 1 : 0;
+    }
+    flags[r] = f;
+}
+
+__global__ void tile_scatter_kernel(const int *__restrict__ flags, const int *__restrict__ idx, int rows,
+                                    int *__restrict__ tiles) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r > rows) return;
+    if (flags[r]) tiles[idx[r]] = r;
+}
+
+__global__ void iota_kernel(int *__restrict__ a, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        a[i] = static_cast<int>(i);
+}
+
+__global__ void count_cols_kernel(const int *__restrict__ ci, int64_t nnz, int *__restrict__ cnt) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(cnt + ci[k] + 1, 1);
+}
+
+__global__ void expand_rows_kernel(const int *__restrict__ ro, int rows, int *__restrict__ rowidx) {
+    // one warp per row
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= rows) return;
+    for (int k = ro[warp] + lane; k < ro[warp + 1]; k += 32) rowidx[k] = warp;
+}
+
+__global__ void gather_rows_kernel(const int *__restrict__ perm, const int *__restrict__ rowidx, int64_t nnz,
+                                   int *__restrict__ out) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nnz; t += (int64_t)gridDim.x * blockDim.x)
+        out[t] = rowidx[perm[t]];
+}
+
+template <class TD, class TS>
+__global__ void gather_values_kernel(const int *__restrict__ perm, const TS *__restrict__ src, TD *__restrict__ dst,
+                                     int64_t nnz) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nnz; t += (int64_t)gridDim.x * blockDim.x)
+        dst[t] = static_cast<TD>(src[perm[t]]);
+}
+
+int grid_for(int64_t n, int threads = 256) {
+    const int64_t b = (n + threads - 1) / threads;
+    return static_cast<int>(b < 148 * 32 ? (b > 0 ? b : 1) : 148 * 32);
+}
+
+int bits_for(int v) {
+    int b = 1;
+    while (b < 31 && (1 << b) <= v) ++b;
+    return b;
+}
+
+} // namespace
+
+void build_tiles(CsrPattern32 &p, cudaStream_t s) {
+    const int rows = p.rows;
+    DevBuf<int> flags(rows + 1), idx(rows + 1);
+    tile_flags_kernel<<<ceil_div(rows + 1, 256), 256, 0, s>>>(p.ro.get(), rows, flags.get());
+    VK_LAUNCH_CHECK();
+    size_t tb = 0;
+    VK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flags.get(), idx.get(), rows + 1, s));
+    DevBuf<unsigned char> tmp(tb > 0 ? tb : 1);
+    VK_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, flags.get(), idx.get(), rows + 1, s));
+    int last_idx = 0, last_flag = 0;
+    VK_CUDA(cudaMemcpyAsync(&last_idx, idx.get() + rows, sizeof(int), cudaMemcpyDeviceToHost, s));
+    VK_CUDA(cudaMemcpyAsync(&last_flag, flags.get() + rows, sizeof(int), cudaMemcpyDeviceToHost, s));
+    VK_CUDA(cudaStreamSynchronize(s));
+    const int count = last_idx + last_flag; // number of boundaries (tiles + 1)
+    p.ntiles = count - 1;
+    p.tiles.reset(count);
+    tile_scatter_kernel<<<ceil_div(rows + 1, 256), 256, 0, s>>>(flags.get(), idx.get(), rows, p.tiles.get());
+    VK_LAUNCH_CHECK();
+    VK_CUDA(cudaStreamSynchronize(s));
+}
+
+void upload_pattern(int64_t rows, int64_t cols, const int64_t *h_ro, const int64_t *h_ci, CsrPattern32 &out,
+                    cudaStream_t s) {
+    const int64_t nnz = h_ro[rows];
+    out.rows = static_cast<int>(rows);
+    out.cols = static_cast<int>(cols);
+    out.nnz = nnz;
+    out.ro.reset(rows + 1);
+    out.ci.reset(nnz > 0 ? nnz : 1);
+    {
+        DevBuf<int64_t> t(rows + 1);
+        VK_CUDA(cudaMemcpyAsync(t.get(), h_ro, (rows + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+        narrow_kernel<<<grid_for(rows + 1), 256, 0, s>>>(t.get(), out.ro.get(), rows + 1);
+        VK_LAUNCH_CHECK();
+        VK_CUDA(cudaStreamSynchronize(s));
+    }
+    if (nnz > 0) {
+        DevBuf<int64_t> t(nnz);
+        VK_CUDA(cudaMemcpyAsync(t.get(), h_ci, nnz * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+        narrow_kernel<<<grid_for(nnz), 256, 0, s>>>(t.get(), out.ci.get(), nnz);
+        VK_LAUNCH_CHECK();
+        VK_CUDA(cudaStreamSynchronize(s));
+    }
+    int mr = 0;
+    for (int64_t r = 0; r < rows; ++r) mr = std::max<int>(mr, static_cast<int>(h_ro[r + 1] - h_ro[r]));
+    out.max_row = mr;
+    build_tiles(out, s);
+}
+
+void expand_rows(const CsrPattern32 &p, int *rowidx, cudaStream_t s) {
+    if (p.rows == 0) return;
+    expand_rows_kernel<<<ceil_div(static_cast<int64_t>(p.rows) * 32, 256), 256, 0, s>>>(p.ro.get(), p.rows, rowidx);
+    VK_LAUNCH_CHECK();
+}
+
+void transpose_pattern(const CsrPattern32 &a, CsrPattern32 &at, DevBuf<int> &perm, cudaStream_t s) {
+    const int64_t nnz = a.nnz;
+    at.rows = a.cols;
+    at.cols = a.rows;
+    at.nnz = nnz;
+    at.ro.reset(a.cols + 1);
+    at.ci.reset(nnz > 0 ? nnz : 1);
+    perm.reset(nnz > 0 ? nnz : 1);
+    VK_CUDA(cudaMemsetAsync(at.ro.get(), 0, (a.cols + 1) * sizeof(int), s));
+    if (nnz > 0) {
+        DevBuf<int> keys_out(nnz), vals_in(nnz), rowidx(nnz);
+        iota_kernel<<<grid_for(nnz), 256, 0, s>>>(vals_in.get(), nnz);
+        VK_LAUNCH_CHECK();
+        const int end_bit = bits_for(a.cols > 0 ? a.cols - 1 : 0);
+        size_t tb = 0;
+        VK_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, a.ci.get(), keys_out.get(), vals_in.get(), perm.get(),
+                                                static_cast<int>(nnz), 0, end_bit, s));
+        DevBuf<unsigned char> tmp(tb > 0 ? tb : 1);
+        VK_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, a.ci.get(), keys_out.get(), vals_in.get(), perm.get(),
+                                                static_cast<int>(nnz), 0, end_bit, s));
+        count_cols_kernel<<<grid_for(nnz), 256, 0, s>>>(a.ci.get(), nnz, at.ro.get());
+        VK_LAUNCH_CHECK();
+        size_t tb2 = 0;
+        VK_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb2, at.ro.get(), at.ro.get(), a.cols + 1, s));
+        DevBuf<unsigned char> tmp2(tb2 > 0 ? tb2 : 1);
+        VK_CUDA(cub::DeviceScan::InclusiveSum(tmp2.get(), tb2, at.ro.get(), at.ro.get(), a.cols + 1, s));
+        expand_rows(a, rowidx.get(), s);
+        gather_rows_kernel<<<grid_for(nnz), 256, 0, s>>>(perm.get(), rowidx.get(), nnz, at.ci.get());
+        VK_LAUNCH_CHECK();
+        VK_CUDA(cudaStreamSynchronize(s));
+    }
+    // longest transposed row
+    {
+        std::vector<int> h(a.cols + 1);
+        VK_CUDA(cudaMemcpyAsync(h.data(), at.ro.get(), (a.cols + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
+        VK_CUDA(cudaStreamSynchronize(s));
+        int mr = 0;
+        for (int j = 0; j < a.cols; ++j) mr = std::max(mr, h[j + 1] - h[j]);
+        at.max_row = mr;
+    }
+    build_tiles(at, s);
+}
+
+template <class TD, class TS>
+void gather_values(const int *perm, const TS *src, TD *dst, int64_t nnz, cudaStream_t s) {
+    if (nnz <= 0) return;
+    gather_values_kernel<TD, TS><<<grid_for(nnz), 256, 0, s>>>(perm, src, dst, nnz);
+    VK_LAUNCH_CHECK();
+}
+
+template void gather_values<double, double>(const int *, const double *, double *, int64_t, cudaStream_t);
+template void gather_values<float, double>(const int *, const double *, float *, int64_t, cudaStream_t);
+template void gather_values<float, float>(const int *, const float *, float *, int64_t, cudaStream_t);
+
+} // namespace vk

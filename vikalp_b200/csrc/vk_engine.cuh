@@ -1,0 +1,43 @@
+// Iteration engines (one per VK_ALGO_*) and the kernels they share.
+#pragma once
+
+#include "vk_solver.h"
+
+#include <chrono>
+
+namespace vk {
+
+struct RunInfo {
+    int status = VK_STATUS_NOT_SOLVED;
+    long long iterations = 0, restarts = 0, fp32_iterations = 0;
+    double last_metric = 0.0;
+    double iterate_seconds = 0.0;
+};
+
+class Engine {
+public:
+    virtual ~Engine() = default;
+    // Runs the iteration for one solve. d_lo / d_hi: effective original
+    // variable bounds; d_warm: warm start in original coordinates or null.
+    // On return d_xo [n] / d_yo [m] hold the answer in original coordinates.
+    virtual void run(const double *d_warm, const double *d_lo, const double *d_hi, double *d_xo, double *d_yo,
+                     RunInfo &info, std::chrono::steady_clock::time_point started) = 0;
+};
+
+std::unique_ptr<Engine> make_reference_engine(const DeviceModel &dm, const vk_options &o, cudaStream_t s);
+std::unique_ptr<Engine> make_halpern_engine(const DeviceModel &dm, const vk_options &o, cudaStream_t s);
+
+// Grid for a one-thread-per-element kernel (no grid-stride loop): covers n.
+inline int grid1d(int64_t n, int threads = 256) {
+    const int64_t b = (n + threads - 1) / threads;
+    return static_cast<int>(b > 0 ? b : 1);
+}
+
+// Deterministic reduction of per-tile partial sums: out[r] = sum_t partials[t*R + r].
+void reduce_partials(const double *partials, int ntiles, int R, double *out, cudaStream_t s);
+
+inline double seconds_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+} // namespace vk

@@ -1,0 +1,446 @@
+// The reference's restarted PDHG / PDQP (pdhg.cpp:87-151, pdqp.cpp:110-178),
+// iterate for iterate, as fused sparse passes with device-side control.
+//
+// One iteration k of the reference is ~30 ExecutionBackend calls (4 SpMVs,
+// 10 copies, 10 axpby, 4 projections, 2 norm_inf with a blocking D2H each).
+// Here it is four kernels and no host round trip:
+//   col     tile pass over the transposed CSR:  aty = K'y_k, and the
+//           stationarity norm of iteration k-1 (pdhg.cpp:122-130), whose
+//           K'y_k is the same product (the reference computes it twice)
+//   control one thread: metric of iteration k-1, the every-50-iterations step
+//           rule (pdhg.cpp:133-145), the stop test, the iteration limit
+//   primal  x_{k+1} = clamp(x_k - tau (c + aty)), xbar (pdhg.cpp:92-104)
+//   row     tile pass over the CSR gathering xbar and x_{k+1} together:
+//           y_{k+1} (pdhg.cpp:105-112) and the primal norm (pdhg.cpp:116-120)
+// (PDQP adds one Q pass after `primal`: Q x_{k+1}, reused by the next
+// iteration's step and stationarity, pdqp.cpp:116,149.)
+// Every floating-point operation keeps the reference's operands and order,
+// with no FMA contraction; with VK_SPMV_SEQUENTIAL the sparse sums are the
+// reference's left-to-right sums too, so iterates match it bit for bit.
+// Chunks of iterations are captured in a CUDA graph; the host only polls a
+// done flag between chunks.
+#include "vk_engine.cuh"
+
+#include <cmath>
+#include <limits>
+
+namespace vk {
+namespace {
+
+// ---- setup kernels (continuous_common.hpp:133-225) --------------------------
+
+// scale[r] = 1/max|v| over row r when that max exceeds 1 (order-free max).
+__global__ void absmax_scale_kernel(const int *__restrict__ ro, const double *__restrict__ v, int rows,
+                                    double *__restrict__ scale) {
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= rows) return;
+    double mx = 0.0;
+    for (int k = ro[r] + lane; k < ro[r + 1]; k += 32) mx = smax(mx, fabs(v[k]));
+    mx = warp_max_nonneg(mx);
+    if (lane == 0) scale[r] = (mx > 1.0) ? 1.0 / mx : 1.0;
+}
+
+// out[k] = v[k] * (rs[row] * cs[col]) (continuous_common.hpp:179-187). For the
+// transposed pattern pass transposed = true: the pattern's rows are columns.
+__global__ void scale_values_kernel(const int *__restrict__ ro, const int *__restrict__ ci,
+                                    const double *__restrict__ v, const double *__restrict__ rs,
+                                    const double *__restrict__ cs, int rows, bool transposed,
+                                    double *__restrict__ out) {
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= rows) return;
+    for (int k = ro[r] + lane; k < ro[r + 1]; k += 32) {
+        const int c = ci[k];
+        const double f = transposed ? __dmul_rn(rs[c], cs[r]) : __dmul_rn(rs[r], cs[c]);
+        out[k] = __dmul_rn(v[k], f);
+    }
+}
+
+// Sequential |v| row sums (the reference's order), max over rows.
+__global__ void abs_rowsum_max_kernel(const int *__restrict__ ro, const double *__restrict__ v, int rows,
+                                      double *__restrict__ out_max) {
+    __shared__ double scratch[32];
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    double s = 0.0;
+    if (r < rows)
+        for (int k = ro[r]; k < ro[r + 1]; ++k) s = __dadd_rn(s, fabs(v[k]));
+    s = block_max_nonneg(s, scratch);
+    if (threadIdx.x == 0) atomic_max_nonneg(out_max, s);
+}
+
+__global__ void scale_vec_kernel(const double *__restrict__ a, const double *__restrict__ sc, int n, bool multiply,
+                                 bool bounds, double *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = a[i];
+    if (bounds && !isfinite(v)) {
+        out[i] = v;
+        return;
+    }
+    out[i] = multiply ? __dmul_rn(v, sc[i]) : __ddiv_rn(v, sc[i]);
+}
+
+// x0 = clamp(warm / cs or 0, l, u) with the scaled bounds (pdhg.cpp:61-72).
+__global__ void ref_prepare_kernel(const double *__restrict__ warm, const double *__restrict__ lo,
+                                   const double *__restrict__ hi, const double *__restrict__ cs, int n,
+                                   double *__restrict__ sl, double *__restrict__ su, double *__restrict__ x) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const double s = cs[j];
+    const double l = isfinite(lo[j]) ? __ddiv_rn(lo[j], s) : lo[j];
+    const double u = isfinite(hi[j]) ? __ddiv_rn(hi[j], s) : hi[j];
+    sl[j] = l;
+    su[j] = u;
+    const double x0 = warm ? __ddiv_rn(warm[j], s) : 0.0;
+    x[j] = clampbox(x0, l, u);
+}
+
+__global__ void unscale_kernel(const double *__restrict__ a, const double *__restrict__ sc, int n,
+                               double *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = __dmul_rn(a[i], sc[i]);
+}
+
+// ---- iteration kernels ------------------------------------------------------
+
+template <bool QP>
+struct RefColEpi : EpiBase<double> {
+    RefCtl *ctl;
+    double *aty;
+    const double *x, *c, *l, *u, *qx;
+    __device__ bool skip() const { return ctl->done != 0; }
+    __device__ void row(int j, const double (&s)[1], double (&red)[1]) const {
+        aty[j] = s[0];
+        if (ctl->iter >= 1) {
+            const double g = QP ? __dadd_rn(s[0], __dadd_rn(c[j], qx[j])) : __dadd_rn(s[0], c[j]);
+            const double xj = x[j];
+            const double px = clampbox(__dadd_rn(-g, xj), l[j], u[j]);
+            red[0] = smax(red[0], fabs(__dadd_rn(-px, xj)));
+        }
+    }
+    __device__ void finish(double (&red)[1], double *scratch, int) const {
+        const double v = block_max_nonneg(red[0], scratch);
+        if (threadIdx.x == 0) atomic_max_nonneg(&ctl->rd, v);
+    }
+};
+
+struct RefRowEpi : EpiBase<double> {
+    RefCtl *ctl;
+    double *y;
+    const double *rl, *ru;
+    __device__ bool skip() const { return ctl->done != 0; }
+    __device__ void row(int i, const double (&s)[2], double (&red)[1]) const {
+        const double sigma = ctl->sigma, inv = ctl->inv_sigma;
+        const double yarg = __dadd_rn(__dmul_rn(sigma, s[0]), y[i]);
+        const double lo = rl[i], hi = ru[i];
+        const double yp = clampbox(__dmul_rn(inv, yarg), lo, hi);
+        y[i] = __dadd_rn(__dmul_rn(-sigma, yp), yarg);
+        const double pax = clampbox(s[1], lo, hi);
+        red[0] = smax(red[0], fabs(__dadd_rn(pax, -s[1])));
+    }
+    __device__ void finish(double (&red)[1], double *scratch, int tile) const {
+        const double v = block_max_nonneg(red[0], scratch);
+        if (threadIdx.x == 0) {
+            atomic_max_nonneg(&ctl->rp, v);
+            if (tile == 0) atomicAdd(reinterpret_cast<unsigned long long *>(&ctl->iter), 1ull);
+        }
+    }
+};
+
+struct StoreEpi : EpiBase<double> {
+    RefCtl *ctl;
+    double *out;
+    __device__ bool skip() const { return ctl && ctl->done != 0; }
+    __device__ void row(int i, const double (&s)[1], double (&)[1]) const { out[i] = s[0]; }
+};
+
+// The metric of iteration k-1 and the step / restart / stop rules
+// (pdhg.cpp:133-150). One thread.
+__global__ void ref_control_kernel(RefCtl *ctl) {
+    RefCtl c = *ctl;
+    if (c.done) return;
+    c.restart = 0; // consumed by the previous primal step (pdhg.cpp:98-100)
+    if (c.iter >= 1) {
+        const long long it = c.iter - 1;
+        const double metric = smax(c.rp, c.rd);
+        c.last_metric = metric;
+        if (it > 0 && it % 50 == 0) {
+            if (metric > c.previous * 1.25) {
+                c.tau *= 0.5;
+                c.sigma *= 0.5;
+                c.restart = 1;
+                c.restarts += 1;
+            } else if (metric < c.previous * 0.1) {
+                c.tau = smin(c.tau * 1.05, c.max_step);
+                c.sigma = c.tau;
+            }
+            c.previous = metric;
+        } else if (it == 0) {
+            c.previous = metric;
+        }
+        if (metric <= c.tol) {
+            c.done = 1;
+            c.status = VK_STATUS_OPTIMAL;
+        }
+    }
+    if (!c.done && c.iter >= c.limit) {
+        c.done = 1;
+        c.status = VK_STATUS_ITERATION_LIMIT;
+    }
+    c.inv_sigma = 1.0 / c.sigma;
+    c.rp = 0.0;
+    c.rd = 0.0;
+    *ctl = c;
+}
+
+template <bool QP>
+__global__ void ref_primal_kernel(const RefCtl *__restrict__ ctl, const double *__restrict__ x,
+                                  const double *__restrict__ aty, const double *__restrict__ c,
+                                  const double *__restrict__ qx, const double *__restrict__ l,
+                                  const double *__restrict__ u, int n, double *__restrict__ xn,
+                                  double *__restrict__ xbar) {
+    if (ctl->done) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const double tau = ctl->tau;
+    const double xj = x[j];
+    double v;
+    if (QP) {
+        const double g = __dadd_rn(aty[j], __dadd_rn(c[j], qx[j]));
+        v = __dadd_rn(__dmul_rn(-tau, g), xj);
+    } else {
+        const double t = __dadd_rn(__dmul_rn(-tau, c[j]), xj);
+        v = __dadd_rn(__dmul_rn(-tau, aty[j]), t);
+    }
+    v = clampbox(v, l[j], u[j]);
+    xn[j] = v;
+    xbar[j] = ctl->restart ? v : __dadd_rn(__dmul_rn(2.0, v), -xj);
+}
+
+class ReferenceEngine final : public Engine {
+public:
+    ReferenceEngine(const DeviceModel &dm, const vk_options &o, cudaStream_t s)
+        : dm_(dm), o_(o), s_(s), exact_(o.spmv_order == VK_SPMV_SEQUENTIAL) {
+        const int m = dm.m, n = dm.n;
+        rs_.reset(m > 0 ? m : 1);
+        cs_.reset(n);
+        ka_.reset(dm.nnz > 0 ? dm.nnz : 1);
+        kat_.reset(dm.nnz > 0 ? dm.nnz : 1);
+        sc_.reset(n);
+        srl_.reset(m > 0 ? m : 1);
+        sru_.reset(m > 0 ? m : 1);
+        // Scale factors on the original values (continuous_common.hpp:149-176).
+        if (m > 0)
+            absmax_scale_kernel<<<ceil_div(int64_t(m) * 32, 256), 256, 0, s>>>(dm.a.ro.get(), dm.a_val.get(), m,
+                                                                                rs_.get());
+        absmax_scale_kernel<<<ceil_div(int64_t(n) * 32, 256), 256, 0, s>>>(dm.at.ro.get(), dm.at_val.get(), n,
+                                                                            cs_.get());
+        VK_LAUNCH_CHECK();
+        if (m > 0)
+            scale_values_kernel<<<ceil_div(int64_t(m) * 32, 256), 256, 0, s>>>(
+                dm.a.ro.get(), dm.a.ci.get(), dm.a_val.get(), rs_.get(), cs_.get(), m, false, ka_.get());
+        scale_values_kernel<<<ceil_div(int64_t(n) * 32, 256), 256, 0, s>>>(
+            dm.at.ro.get(), dm.at.ci.get(), dm.at_val.get(), rs_.get(), cs_.get(), n, true, kat_.get());
+        VK_LAUNCH_CHECK();
+        scale_vec_kernel<<<grid1d(n), 256, 0, s>>>(dm.c.get(), cs_.get(), n, true, false, sc_.get());
+        if (m > 0) {
+            scale_vec_kernel<<<grid1d(m), 256, 0, s>>>(dm.rl.get(), rs_.get(), m, true, true, srl_.get());
+            scale_vec_kernel<<<grid1d(m), 256, 0, s>>>(dm.ru.get(), rs_.get(), m, true, true, sru_.get());
+        }
+        VK_LAUNCH_CHECK();
+        // Step size (pdhg.cpp:75-78, pdqp.cpp:89-99).
+        DevBuf<double> mx(3);
+        VK_CUDA(cudaMemsetAsync(mx.get(), 0, 3 * sizeof(double), s));
+        if (m > 0)
+            abs_rowsum_max_kernel<<<ceil_div(m, 256), 256, 0, s>>>(dm.a.ro.get(), ka_.get(), m, mx.get());
+        abs_rowsum_max_kernel<<<ceil_div(n, 256), 256, 0, s>>>(dm.at.ro.get(), kat_.get(), n, mx.get() + 1);
+        VK_LAUNCH_CHECK();
+        if (dm.qp) {
+            kq_.reset(dm.q_nnz);
+            scale_values_kernel<<<ceil_div(int64_t(n) * 32, 256), 256, 0, s>>>(
+                dm.q.ro.get(), dm.q.ci.get(), dm.q_val.get(), cs_.get(), cs_.get(), n, false, kq_.get());
+            abs_rowsum_max_kernel<<<ceil_div(n, 256), 256, 0, s>>>(dm.q.ro.get(), kq_.get(), n, mx.get() + 2);
+            VK_LAUNCH_CHECK();
+        }
+        double h[3];
+        VK_CUDA(cudaMemcpyAsync(h, mx.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+        VK_CUDA(cudaStreamSynchronize(s));
+        const double norm = std::sqrt(h[0] * h[1]);
+        max_step_ = dm.qp ? 0.99 / smax(1.0, norm * norm + h[2]) : 0.99 / smax(1.0, norm);
+        // Iterates.
+        x_[0].reset(n);
+        x_[1].reset(n);
+        xbar_.reset(n);
+        aty_.reset(n);
+        y_.reset(m > 0 ? m : 1);
+        qx_.reset(dm.qp ? n : 1);
+        sl_.reset(n);
+        su_.reset(n);
+        ctl_.reset(1);
+        hctl_.reset(1);
+        // Iterations per graph chunk: enough to amortise the poll, few enough
+        // to stop promptly.
+        const int64_t work = dm.nnz + dm.m + dm.n;
+        chunk_ = work < (1 << 20) ? 64 : (work < (1 << 24) ? 16 : 4);
+    }
+
+    ~ReferenceEngine() override {
+        if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    }
+
+    void run(const double *d_warm, const double *d_lo, const double *d_hi, double *d_xo, double *d_yo,
+             RunInfo &info, std::chrono::steady_clock::time_point started) override {
+        const int m = dm_.m, n = dm_.n;
+        ref_prepare_kernel<<<grid1d(n), 256, 0, s_>>>(d_warm, d_lo, d_hi, cs_.get(), n, sl_.get(), su_.get(),
+                                                      x_[0].get());
+        VK_LAUNCH_CHECK();
+        if (m > 0) VK_CUDA(cudaMemsetAsync(y_.get(), 0, m * sizeof(double), s_));
+        if (dm_.qp) q_product(x_[0].get(), nullptr);
+        RefCtl c{};
+        c.tau = c.sigma = max_step_;
+        c.inv_sigma = 1.0 / c.sigma;
+        c.max_step = max_step_;
+        c.previous = std::numeric_limits<double>::infinity();
+        c.last_metric = std::numeric_limits<double>::quiet_NaN();
+        c.tol = smax(o_.primal_tolerance, o_.dual_tolerance);
+        c.limit = o_.iteration_limit;
+        c.status = VK_STATUS_NOT_SOLVED;
+        VK_CUDA(cudaMemcpyAsync(ctl_.get(), &c, sizeof(c), cudaMemcpyHostToDevice, s_));
+        if (!graph_exec_) capture();
+        cudaEvent_t e0, e1;
+        VK_CUDA(cudaEventCreate(&e0));
+        VK_CUDA(cudaEventCreate(&e1));
+        VK_CUDA(cudaEventRecord(e0, s_));
+        bool timed_out = false;
+        for (;;) {
+            if (std::isfinite(o_.time_limit_seconds) && seconds_since(started) >= o_.time_limit_seconds) {
+                timed_out = true;
+                break;
+            }
+            VK_CUDA(cudaGraphLaunch(graph_exec_, s_));
+            VK_CUDA(cudaMemcpyAsync(hctl_.get(), ctl_.get(), sizeof(RefCtl), cudaMemcpyDeviceToHost, s_));
+            VK_CUDA(cudaStreamSynchronize(s_));
+            if (hctl_[0].done) break;
+        }
+        VK_CUDA(cudaEventRecord(e1, s_));
+        VK_CUDA(cudaMemcpyAsync(hctl_.get(), ctl_.get(), sizeof(RefCtl), cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaStreamSynchronize(s_));
+        float ms = 0.f;
+        VK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        const RefCtl &h = hctl_[0];
+        info.iterations = h.iter;
+        info.restarts = h.restarts;
+        info.last_metric = h.last_metric;
+        info.status = timed_out && !h.done ? VK_STATUS_TIME_LIMIT : h.status;
+        info.iterate_seconds = ms * 1e-3;
+        const double *xf = x_[h.iter % 2].get();
+        unscale_kernel<<<grid1d(n), 256, 0, s_>>>(xf, cs_.get(), n, d_xo);
+        if (m > 0) unscale_kernel<<<grid1d(m), 256, 0, s_>>>(y_.get(), rs_.get(), m, d_yo);
+        VK_LAUNCH_CHECK();
+    }
+
+private:
+    template <class Epi, int NV>
+    void tiles(const CsrView<double> &M, const Gathers<double, NV> &g, const Epi &e) {
+        if (exact_)
+            launch_tiles<double, double, NV, true>(M, g, e, s_);
+        else
+            launch_tiles<double, double, NV, false>(M, g, e, s_);
+    }
+
+    void q_product(const double *x, RefCtl *ctl) {
+        StoreEpi e;
+        e.ctl = ctl;
+        e.out = qx_.get();
+        tiles(view(dm_.q, kq_.get()), Gathers<double, 1>{{x}}, e);
+    }
+
+    void iteration(int k) {
+        const int n = dm_.n;
+        double *cur = x_[k % 2].get(), *nxt = x_[(k + 1) % 2].get();
+        if (dm_.qp) {
+            RefColEpi<true> e;
+            fill_col(e, cur);
+            tiles(view(dm_.at, kat_.get()), Gathers<double, 1>{{y_.get()}}, e);
+        } else {
+            RefColEpi<false> e;
+            fill_col(e, cur);
+            tiles(view(dm_.at, kat_.get()), Gathers<double, 1>{{y_.get()}}, e);
+        }
+        ref_control_kernel<<<1, 1, 0, s_>>>(ctl_.get());
+        VK_LAUNCH_CHECK();
+        if (dm_.qp)
+            ref_primal_kernel<true><<<grid1d(n), 256, 0, s_>>>(ctl_.get(), cur, aty_.get(), sc_.get(), qx_.get(),
+                                                               sl_.get(), su_.get(), n, nxt, xbar_.get());
+        else
+            ref_primal_kernel<false><<<grid1d(n), 256, 0, s_>>>(ctl_.get(), cur, aty_.get(), sc_.get(), nullptr,
+                                                                sl_.get(), su_.get(), n, nxt, xbar_.get());
+        VK_LAUNCH_CHECK();
+        if (dm_.qp) q_product(nxt, ctl_.get());
+        RefRowEpi r;
+        r.ctl = ctl_.get();
+        r.y = y_.get();
+        r.rl = srl_.get();
+        r.ru = sru_.get();
+        if (dm_.m > 0) {
+            tiles(view(dm_.a, ka_.get()), Gathers<double, 2>{{xbar_.get(), nxt}}, r);
+        } else {
+            // No rows: the iteration still completes.
+            bump_iter_kernel_launch();
+        }
+    }
+
+    template <class E>
+    void fill_col(E &e, double *cur) {
+        e.ctl = ctl_.get();
+        e.aty = aty_.get();
+        e.x = cur;
+        e.c = sc_.get();
+        e.l = sl_.get();
+        e.u = su_.get();
+        e.qx = qx_.get();
+    }
+
+    void bump_iter_kernel_launch();
+
+    void capture() {
+        VK_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < 2 * chunk_; ++k) iteration(k);
+        cudaGraph_t g;
+        VK_CUDA(cudaStreamEndCapture(s_, &g));
+        VK_CUDA(cudaGraphInstantiate(&graph_exec_, g, 0));
+        cudaGraphDestroy(g);
+    }
+
+    const DeviceModel &dm_;
+    vk_options o_;
+    cudaStream_t s_;
+    bool exact_;
+    DevBuf<double> rs_, cs_, ka_, kat_, kq_, sc_, srl_, sru_;
+    DevBuf<double> x_[2], xbar_, aty_, y_, qx_, sl_, su_;
+    DevBuf<RefCtl> ctl_;
+    HostBuf<RefCtl> hctl_;
+    double max_step_ = 0.0;
+    int chunk_ = 16;
+    cudaGraphExec_t graph_exec_ = nullptr;
+};
+
+__global__ void bump_iter_kernel(RefCtl *ctl) {
+    if (!ctl->done) ctl->iter += 1;
+}
+
+void ReferenceEngine::bump_iter_kernel_launch() {
+    bump_iter_kernel<<<1, 1, 0, s_>>>(ctl_.get());
+    VK_LAUNCH_CHECK();
+}
+
+} // namespace
+
+std::unique_ptr<Engine> make_reference_engine(const DeviceModel &dm, const vk_options &o, cudaStream_t s) {
+    return std::make_unique<ReferenceEngine>(dm, o, s);
+}
+
+} // namespace vk

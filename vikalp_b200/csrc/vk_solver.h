@@ -1,0 +1,70 @@
+// Host-side declarations of the PDHG solver objects behind the C ABI.
+#pragma once
+
+#include "vikalp_b200.h"
+#include "vk_csr.cuh"
+
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace vk {
+
+// The model as uploaded once by vk_pdhg_create (original coordinates, FP64).
+struct DeviceModel {
+    int m = 0, n = 0;
+    int64_t nnz = 0, q_nnz = 0;
+    bool qp = false;
+    CsrPattern32 a, at, q;
+    DevBuf<int> perm;               // transposed position -> CSR position
+    DevBuf<double> a_val, at_val;   // original values, CSR and transposed order
+    DevBuf<double> q_val;           // original Q values (full symmetric CSR)
+    DevBuf<double> c, vl, vu, rl, ru;
+    double offset = 0.0;
+    std::vector<double> h_c;                 // for the host-side objective sum
+    std::vector<int64_t> h_qro, h_qci;       // Q on the host (objective's quadratic term)
+    std::vector<double> h_qv;
+    std::vector<double> h_vl, h_vu;          // model bounds (override validation)
+};
+
+// Device control block of the reference scheme (pdhg.cpp:75-150).
+struct RefCtl {
+    double tau, sigma, inv_sigma, max_step;
+    double previous, last_metric, tol;
+    double rp, rd; // atomic-max slots for the two infinity norms
+    long long iter, limit, restarts;
+    int restart, done, status, pad;
+};
+
+// Final-answer reductions of the post-processing passes.
+struct PostOut {
+    double primal_res, stat_res, comp_res;            // infinity norms (atomic max)
+    double sums[12];                                  // relative-KKT sums (see vk_pdhg.cu)
+};
+
+class Engine;
+
+class Solver {
+public:
+    Solver(const vk_problem &p, const vk_options &o);
+    ~Solver();
+    void solve(const double *warm, const double *lo, const double *hi, vk_result *r);
+    const DeviceModel &model() const { return *dm_; }
+    cudaStream_t stream() const { return stream_; }
+
+private:
+    vk_options opts_;
+    cudaStream_t stream_ = nullptr;
+    std::unique_ptr<DeviceModel> dm_;
+    std::unique_ptr<Engine> engine_;
+};
+
+// Validation of a vk_problem with the reference's rules and messages.
+// Returns "" when valid. `unsupported` is set when the failure maps to
+// SolveStatus::UnsupportedModel instead of InvalidModel.
+std::string validate_problem(const vk_problem &p, const vk_options &o, bool &unsupported);
+
+// Uploads a validated problem.
+std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s);
+
+} // namespace vk
