@@ -86,6 +86,8 @@ _SIGNATURES = {
     "vk_spmat_create": (C.c_int, [C.POINTER(Csr), C.c_int32, C.POINTER(C.c_void_p)]),
     "vk_spmat_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "vk_spmat_bytes": (C.c_int64, [C.c_void_p, C.c_int]),
+    "vk_spmat_variant": (C.c_int, [C.c_void_p, C.c_int]),
+    "vk_spmat_set_variant": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "vk_spmat_destroy": (None, [C.c_void_p]),
 }
 
@@ -265,6 +267,12 @@ class SpMat:
 
     def bytes(self, transpose: bool = False) -> int:
         return int(lib().vk_spmat_bytes(self._h, int(transpose)))
+
+    def variant(self, transpose: bool = False) -> int:
+        return int(lib().vk_spmat_variant(self._h, int(transpose)))
+
+    def set_variant(self, variant: int, transpose: bool = False):
+        _check(lib().vk_spmat_set_variant(self._h, int(transpose), int(variant)))
 
     def close(self):
         if getattr(self, "_h", None):

@@ -61,13 +61,13 @@ void check_csr(const vk_csr *a) {
 }
 
 template <class T>
-struct PlainEpi : vk::EpiBase<T> {
+struct PlainEpi : vk::EpiRow<T, PlainEpi<T>> {
     T *y;
     __device__ void row(int i, const T (&s)[1], double (&)[1]) const { y[i] = s[0]; }
 };
 
 // y = alpha * acc + beta * y (cpu_ops.cpp:426)
-struct AxpbyEpi : vk::EpiBase<double> {
+struct AxpbyEpi : vk::EpiRow<double, AxpbyEpi> {
     double alpha, beta;
     double *y;
     __device__ void row(int i, const double (&s)[1], double (&)[1]) const {
@@ -76,7 +76,7 @@ struct AxpbyEpi : vk::EpiBase<double> {
 };
 
 // y *= beta, then y[col] += v * (alpha * x[row]) in row order (cpu_ops.cpp:444-458)
-struct ScatterEpi : vk::EpiBase<double> {
+struct ScatterEpi : vk::EpiRow<double, ScatterEpi> {
     double alpha, beta;
     double *y;
     __device__ double init(int j, int) const { return __dmul_rn(beta, y[j]); }
@@ -205,7 +205,7 @@ int vk_spmv(const vk_csr *a, double alpha, const double *x, double beta, double 
         vk::upload_pattern(a->rows, a->cols, a->rows > 0 ? a->row_offsets : &zero, a->col_indices, p, st.s);
         const int64_t nnz = p.nnz;
         const int64_t xl = transpose ? a->rows : a->cols, yl = transpose ? a->cols : a->rows;
-        vk::DevBuf<double> v(nnz > 0 ? nnz : 1), dx(xl > 0 ? xl : 1), dy(yl > 0 ? yl : 1);
+        vk::DevBuf<double> v(vk::padded(nnz)), dx(xl > 0 ? xl : 1), dy(yl > 0 ? yl : 1);
         if (nnz > 0) VK_CUDA(cudaMemcpyAsync(v.get(), a->values, nnz * sizeof(double), cudaMemcpyHostToDevice, st.s));
         if (xl > 0) VK_CUDA(cudaMemcpyAsync(dx.get(), x, xl * sizeof(double), cudaMemcpyHostToDevice, st.s));
         if (yl > 0) VK_CUDA(cudaMemcpyAsync(dy.get(), y, yl * sizeof(double), cudaMemcpyHostToDevice, st.s));
@@ -224,7 +224,7 @@ int vk_spmv(const vk_csr *a, double alpha, const double *x, double beta, double 
             vk::CsrPattern32 pt;
             vk::DevBuf<int> pm;
             vk::transpose_pattern(p, pt, pm, st.s);
-            vk::DevBuf<double> tv(nnz > 0 ? nnz : 1);
+            vk::DevBuf<double> tv(vk::padded(nnz));
             vk::gather_values<double, double>(pm.get(), v.get(), tv.get(), nnz, st.s);
             ScatterEpi e;
             e.alpha = alpha;
@@ -238,6 +238,7 @@ int vk_spmv(const vk_csr *a, double alpha, const double *x, double beta, double 
         }
         if (yl > 0) VK_CUDA(cudaMemcpyAsync(y, dy.get(), yl * sizeof(double), cudaMemcpyDeviceToHost, st.s));
         VK_CUDA(cudaStreamSynchronize(st.s));
+        vk::check_device_error(st.s);
         return VK_OK;
     });
 }
@@ -255,24 +256,24 @@ int vk_spmat_create(const vk_csr *a, int32_t precision, vk_spmat **out) {
         vk::upload_pattern(a->rows, a->cols, a->rows > 0 ? a->row_offsets : &zero, a->col_indices, h->a, st.s);
         const int64_t nnz = h->a.nnz;
         vk::transpose_pattern(h->a, h->at, h->perm, st.s);
-        vk::DevBuf<double> v(nnz > 0 ? nnz : 1);
+        vk::DevBuf<double> v(vk::padded(nnz));
         if (nnz > 0) VK_CUDA(cudaMemcpyAsync(v.get(), a->values, nnz * sizeof(double), cudaMemcpyHostToDevice, st.s));
         if (precision == VK_PREC_FP64) {
-            h->vt64.reset(nnz > 0 ? nnz : 1);
+            h->vt64.reset(vk::padded(nnz));
             vk::gather_values<double, double>(h->perm.get(), v.get(), h->vt64.get(), nnz, st.s);
             h->v64 = std::move(v);
         } else {
-            h->v32.reset(nnz > 0 ? nnz : 1);
-            h->vt32.reset(nnz > 0 ? nnz : 1);
-            vk::DevBuf<int> iota;
-            // CSR order: v32[k] = v[k]
-            std::vector<int> id(nnz > 0 ? nnz : 1);
-            for (int64_t k = 0; k < nnz; ++k) id[k] = static_cast<int>(k);
-            iota.reset(id.size());
-            VK_CUDA(cudaMemcpyAsync(iota.get(), id.data(), id.size() * sizeof(int), cudaMemcpyHostToDevice, st.s));
-            vk::gather_values<float, double>(iota.get(), v.get(), h->v32.get(), nnz, st.s);
+            h->v32.reset(vk::padded(nnz));
+            h->vt32.reset(vk::padded(nnz));
+            vk::convert_values<float, double>(v.get(), h->v32.get(), nnz, st.s);
             vk::gather_values<float, double>(h->perm.get(), v.get(), h->vt32.get(), nnz, st.s);
-            VK_CUDA(cudaStreamSynchronize(st.s));
+        }
+        if (precision == VK_PREC_FP64) {
+            vk::autotune_pattern<double>(h->a, h->v64.get(), st.s);
+            vk::autotune_pattern<double>(h->at, h->vt64.get(), st.s);
+        } else {
+            vk::autotune_pattern<float>(h->a, h->v32.get(), st.s);
+            vk::autotune_pattern<float>(h->at, h->vt32.get(), st.s);
         }
         VK_CUDA(cudaStreamSynchronize(st.s));
         *out = h.release();
@@ -305,6 +306,18 @@ int64_t vk_spmat_bytes(const vk_spmat *m, int transpose) {
     const vk::CsrPattern32 &p = transpose ? m->at : m->a;
     const int64_t s = m->precision == VK_PREC_FP64 ? 8 : 4;
     return p.nnz * (s + 4) + 4 * (int64_t(p.rows) + 1) + int64_t(p.cols) * s + int64_t(p.rows) * s;
+}
+
+int vk_spmat_variant(const vk_spmat *m, int transpose) {
+    if (!m) return -1;
+    return transpose ? m->at.variant : m->a.variant;
+}
+
+int vk_spmat_set_variant(vk_spmat *m, int transpose, int variant) {
+    if (!m || variant < 0 || variant >= vk::kFastVariants)
+        return set_error(VK_ERR_INVALID, "variant out of range");
+    (transpose ? m->at : m->a).variant = variant;
+    return VK_OK;
 }
 
 void vk_spmat_destroy(vk_spmat *m) {

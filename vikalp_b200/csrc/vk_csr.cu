@@ -26,9 +26,9 @@ __global__ void tile_flags_kernel(const int *__restrict__ ro, int rows, int *__r
         f = 1;
     } else {
         const int a = ro[r - 1], b = ro[r], c = ro[r + 1];
-        const bool long_prev = (b - a) > kHalfTile;
-        const bool long_here = (c - b) > kHalfTile;
-        f = (long_prev || long_here || (a / kHalfTile) != (b / kHalfTile) || (r % kRowsMax) == 0) ? 1 : 0;
+        const bool long_prev = (b - a) > kShortMax;
+        const bool long_here = (c - b) > kShortMax;
+        f = (long_prev || long_here || (a / kChunk) != (b / kChunk) || (r % kTileRows) == 0) ? 1 : 0;
     }
     flags[r] = f;
 }
@@ -64,6 +64,18 @@ __global__ void gather_rows_kernel(const int *__restrict__ perm, const int *__re
         out[t] = rowidx[perm[t]];
 }
 
+__global__ void tile_k_kernel(const int *__restrict__ ro, const int *__restrict__ tiles, int count,
+                              int *__restrict__ tile_k) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count) tile_k[t] = ro[tiles[t]];
+}
+
+template <class TD, class TS>
+__global__ void convert_values_kernel(const TS *__restrict__ src, TD *__restrict__ dst, int64_t n) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        dst[t] = static_cast<TD>(src[t]);
+}
+
 template <class TD, class TS>
 __global__ void gather_values_kernel(const int *__restrict__ perm, const TS *__restrict__ src, TD *__restrict__ dst,
                                      int64_t nnz) {
@@ -84,6 +96,33 @@ int bits_for(int v) {
 
 } // namespace
 
+int *device_error_flag() {
+    static int *flags[64] = {nullptr};
+    int dev = 0;
+    VK_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw CudaFailure("device ordinal out of range");
+    if (!flags[dev]) {
+        int *p = nullptr;
+        VK_CUDA(cudaMalloc(&p, sizeof(int)));
+        VK_CUDA(cudaMemset(p, 0, sizeof(int)));
+        flags[dev] = p;
+    }
+    return flags[dev];
+}
+
+void check_device_error(cudaStream_t s) {
+    int *f = device_error_flag();
+    int h = 0;
+    VK_CUDA(cudaMemcpyAsync(&h, f, sizeof(int), cudaMemcpyDeviceToHost, s));
+    VK_CUDA(cudaStreamSynchronize(s));
+    if (h != 0) {
+        VK_CUDA(cudaMemsetAsync(f, 0, sizeof(int), s));
+        VK_CUDA(cudaStreamSynchronize(s));
+        throw CudaFailure(h == kDevErrBarrierTimeout ? "a sparse pass timed out waiting for its staged tile"
+                                                     : "a kernel reported a device error");
+    }
+}
+
 void build_tiles(CsrPattern32 &p, cudaStream_t s) {
     const int rows = p.rows;
     DevBuf<int> flags(rows + 1), idx(rows + 1);
@@ -102,17 +141,22 @@ void build_tiles(CsrPattern32 &p, cudaStream_t s) {
     p.tiles.reset(count);
     tile_scatter_kernel<<<ceil_div(rows + 1, 256), 256, 0, s>>>(flags.get(), idx.get(), rows, p.tiles.get());
     VK_LAUNCH_CHECK();
+    p.tile_k.reset(count);
+    tile_k_kernel<<<ceil_div(count, 256), 256, 0, s>>>(p.ro.get(), p.tiles.get(), count, p.tile_k.get());
+    VK_LAUNCH_CHECK();
     VK_CUDA(cudaStreamSynchronize(s));
 }
 
 void upload_pattern(int64_t rows, int64_t cols, const int64_t *h_ro, const int64_t *h_ci, CsrPattern32 &out,
                     cudaStream_t s) {
     const int64_t nnz = h_ro[rows];
+    device_error_flag(); // allocate before any kernel (or graph capture) needs it
     out.rows = static_cast<int>(rows);
     out.cols = static_cast<int>(cols);
     out.nnz = nnz;
     out.ro.reset(rows + 1);
-    out.ci.reset(nnz > 0 ? nnz : 1);
+    out.ci.reset(padded(nnz));
+    VK_CUDA(cudaMemsetAsync(out.ci.get(), 0, padded(nnz) * sizeof(int), s));
     {
         DevBuf<int64_t> t(rows + 1);
         VK_CUDA(cudaMemcpyAsync(t.get(), h_ro, (rows + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
@@ -145,7 +189,8 @@ void transpose_pattern(const CsrPattern32 &a, CsrPattern32 &at, DevBuf<int> &per
     at.cols = a.rows;
     at.nnz = nnz;
     at.ro.reset(a.cols + 1);
-    at.ci.reset(nnz > 0 ? nnz : 1);
+    at.ci.reset(padded(nnz));
+    VK_CUDA(cudaMemsetAsync(at.ci.get(), 0, padded(nnz) * sizeof(int), s));
     perm.reset(nnz > 0 ? nnz : 1);
     VK_CUDA(cudaMemsetAsync(at.ro.get(), 0, (a.cols + 1) * sizeof(int), s));
     if (nnz > 0) {
@@ -189,8 +234,74 @@ void gather_values(const int *perm, const TS *src, TD *dst, int64_t nnz, cudaStr
     VK_LAUNCH_CHECK();
 }
 
+template <class TD, class TS>
+void convert_values(const TS *src, TD *dst, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    convert_values_kernel<TD, TS><<<grid_for(n), 256, 0, s>>>(src, dst, n);
+    VK_LAUNCH_CHECK();
+}
+
+template void convert_values<float, double>(const double *, float *, int64_t, cudaStream_t);
+template void convert_values<double, float>(const float *, double *, int64_t, cudaStream_t);
+template void convert_values<double, double>(const double *, double *, int64_t, cudaStream_t);
+
 template void gather_values<double, double>(const int *, const double *, double *, int64_t, cudaStream_t);
 template void gather_values<float, double>(const int *, const double *, float *, int64_t, cudaStream_t);
 template void gather_values<float, float>(const int *, const float *, float *, int64_t, cudaStream_t);
+
+// ---- autotuner ----------------------------------------------------------------
+namespace {
+template <class T>
+struct TuneEpi : EpiRow<T, TuneEpi<T>> {
+    T *y;
+    __device__ void row(int i, const T (&s)[1], double (&)[1]) const { y[i] = s[0]; }
+};
+
+template <class T>
+__global__ void fill_kernel(T *a, int64_t n, T v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        a[i] = v;
+}
+} // namespace
+
+template <class T>
+void autotune_pattern(CsrPattern32 &p, const T *val, cudaStream_t s, int64_t min_nnz) {
+    p.variant = 0;
+    if (p.nnz < min_nnz || p.rows == 0 || p.cols == 0) return;
+    DevBuf<T> x(p.cols), y(p.rows);
+    fill_kernel<T><<<grid_for(p.cols), 256, 0, s>>>(x.get(), p.cols, T(1));
+    VK_LAUNCH_CHECK();
+    TuneEpi<T> e;
+    e.y = y.get();
+    cudaEvent_t a, b;
+    VK_CUDA(cudaEventCreate(&a));
+    VK_CUDA(cudaEventCreate(&b));
+    float best = 1e30f;
+    int best_v = 0;
+    for (int v = 0; v < kFastVariants; ++v) {
+        p.variant = v;
+        const CsrView<T> M = view(p, val);
+        launch_tiles<T, T, 1, false>(M, Gathers<T, 1>{{x.get()}}, e, s); // warm-up
+        float times[3];
+        for (float &t : times) {
+            VK_CUDA(cudaEventRecord(a, s));
+            launch_tiles<T, T, 1, false>(M, Gathers<T, 1>{{x.get()}}, e, s);
+            VK_CUDA(cudaEventRecord(b, s));
+            VK_CUDA(cudaEventSynchronize(b));
+            VK_CUDA(cudaEventElapsedTime(&t, a, b));
+        }
+        std::sort(times, times + 3);
+        if (times[1] < best) {
+            best = times[1];
+            best_v = v;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    p.variant = best_v;
+}
+
+template void autotune_pattern<double>(CsrPattern32 &, const double *, cudaStream_t, int64_t);
+template void autotune_pattern<float>(CsrPattern32 &, const float *, cudaStream_t, int64_t);
 
 } // namespace vk

@@ -1,40 +1,67 @@
-// Device CSR storage and the tile-stream sparse pass used by every product.
+// Device CSR storage and the sparse passes used by every product.
 //
 // Layout in HBM (per matrix): int32 row offsets [rows+1], int32 column indices
-// [nnz], values [nnz] (float64 or float32), and an int32 tile schedule
-// [ntiles+1] of row starts. A tile is either
-//   * a run of consecutive rows holding at most kNzTile nonzeros and at most
-//     kRowsMax rows, or
-//   * one row longer than kNzTile / 2 ("long row").
-// One CTA streams one tile: the nonzeros of the tile are contiguous in memory,
-// so column indices and values are read fully coalesced, the gathers of x are
-// all independent, and the products land in shared memory. Rows are then
-// summed from shared memory -- one thread per row, left to right (the
-// reference CPU order, cpu_ops.cpp:418-427) for short rows, one warp per row
-// for rows longer than kShortRow -- and handed to a fused epilogue (the PDHG
-// primal or dual update, a residual, ...), so no product vector is written
-// back to HBM.
+// [nnz], values [nnz] (float64 or float32) -- both padded by kPad elements --
+// and a schedule of warp-tiles: tiles[t] = first row, tile_k[t] = first
+// nonzero (ntiles+1 entries each). A warp-tile is either
+//   * a run of at most kTileRows consecutive rows whose row starts fall in the
+//     same kChunk-sized window of the nonzero array and that are each at most
+//     kShortMax long (so it holds at most kChunk - 1 + kShortMax = kCap
+//     nonzeros), or
+//   * one row longer than kShortMax.
+//
+// FAST order (tile_kernel_fast): each warp of a persistent grid walks its own
+// sequence of tiles. Per tile, a short prologue loads the tile's row offsets
+// and the epilogue's per-row inputs (y, bounds, ...) into a small
+// warp-private shared-memory area and marks each row's last nonzero in a
+// bitmask. The warp then streams the tile 32 nonzeros per step, U steps per
+// batch with every load of the batch in flight at once (column indices and
+// values fully coalesced, the gathers of x independent; optionally the next
+// batch's loads issued before this batch is reduced), and forms row sums
+// with a segmented warp scan over the bitmask; the lane holding a row's last
+// nonzero runs the fused epilogue (the PDHG primal or dual update, a
+// residual, ...). No product vector goes back to HBM, there is no CTA-wide
+// barrier in the loop, and only ~40 registers per thread are live, so each
+// SM keeps 48+ warps of loads in flight. Rows longer than kCap are streamed by
+// the whole warp.
+//
+// SEQUENTIAL order (tile_kernel_exact): one thread per row, left to right with
+// each product rounded on its own -- the reference CPU order
+// (cpu_ops.cpp:418-427, 444-458), so results are bit-identical to it. It is
+// the parity mode, not the fast path.
 #pragma once
 
 #include "vk_common.cuh"
 
 namespace vk {
 
-constexpr int kTileThreads = 256;
-constexpr int kNzTile = 2048;            // max nonzeros per multi-row tile
-constexpr int kHalfTile = kNzTile / 2;   // rows longer than this get their own tile
-constexpr int kRowsMax = 512;            // max rows per tile
-constexpr int kShortRow = 32;            // rows up to this length: one thread
-constexpr int kPer = kNzTile / kTileThreads;
+constexpr int kWarps = 4;                  // warps per CTA
+constexpr int kTileThreads = kWarps * 32;  // threads per CTA
+constexpr int kChunk = 768;                // nonzero window that groups short rows
+constexpr int kShortMax = 256;             // longer rows get a tile of their own
+constexpr int kCap = kChunk + kShortMax;   // max nonzeros of a multi-row tile
+constexpr int kTileRows = 64;              // max rows per warp-tile
+constexpr int kPad = 8;                    // padding (elements) of index / value arrays
+constexpr int kMaxGridPerSM = 16;          // persistent CTAs per SM (upper bound)
+constexpr int kMaxGrid = 160 * kMaxGridPerSM; // partial-sum buffers are sized for this
 
-// Owning device CSR pattern + tile schedule (values are stored by the user).
+inline int64_t padded(int64_t nnz) { return nnz + kPad; }
+
+// Owning device CSR pattern + tile schedule (values are stored by the user,
+// padded(nnz) elements).
 struct CsrPattern32 {
     int rows = 0, cols = 0;
     int64_t nnz = 0;
-    DevBuf<int> ro, ci, tiles;
+    DevBuf<int> ro, ci, tiles, tile_k;
     int ntiles = 0;
     int max_row = 0;
+    int variant = 0; // FAST kernel variant picked by autotune_pattern
 };
+
+// Per-device error flag the kernels write (first error wins).
+int *device_error_flag();
+// Reads and clears the flag; throws CudaFailure when a kernel reported one.
+void check_device_error(cudaStream_t s);
 
 // Non-owning views passed to kernels.
 template <class T>
@@ -43,12 +70,16 @@ struct CsrView {
     const int *__restrict__ ci;
     const T *__restrict__ val;
     const int *__restrict__ tiles;
+    const int *__restrict__ tile_k;
+    int *err;
     int rows, cols, ntiles;
+    int variant; // FAST kernel variant (autotuned per matrix)
 };
 
 template <class T>
 inline CsrView<T> view(const CsrPattern32 &p, const T *val) {
-    return CsrView<T>{p.ro.get(), p.ci.get(), val, p.tiles.get(), p.rows, p.cols, p.ntiles};
+    return CsrView<T>{p.ro.get(), p.ci.get(), val, p.tiles.get(), p.tile_k.get(), device_error_flag(),
+                      p.rows, p.cols, p.ntiles, p.variant};
 }
 
 // Rounded multiply / add that the compiler never contracts into an FMA, so the
@@ -63,175 +94,310 @@ struct Gathers {
     const T *__restrict__ p[NV];
 };
 
-// Shared memory of one tile pass.
-template <class A, int NV>
-struct TileSmem {
-    A prod[NV][kNzTile];
-    int rofs[kRowsMax + 1];
-    int long_list[kRowsMax];
-    int n_long;
-    double red[32 * 8];
-};
+// Epilogue interface (EpiBase has defaults for all but row_pre / row):
+//   static constexpr int NR;                            reduction slots (>= 1)
+//   struct Pre; __device__ Pre load(int row) const;     per-row inputs, loaded early
+//   __device__ bool skip() const;                       whole launch is a no-op
+//   __device__ A init(int row, int q) const;            accumulator start value
+//   __device__ A gscale(int q) const;                   factor on gathered values
+//   __device__ void row_pre(int row, const A (&s)[NV], const Pre &, double (&red)[NR]) const;
+//   __device__ void finish(double (&red)[NR], double *scratch, int block) const;
+// row_pre is called exactly once per matrix row with
+//   s[q] = init(row, q) + sum_k v_k * (gscale(q) * x_q[c_k]).
+// finish is called once by every thread of every CTA after its last row; it
+// does the CTA-level reduction itself (scratch: 32*8 doubles of shared memory).
 
-// The tile pass. Epi must provide:
-//   static constexpr int NR;                           reduction slots
-//   __device__ A init(int row, int q) const;           accumulator start value
-//   __device__ A gscale(int q) const;                  factor on gathered values (1 = none)
-//   __device__ void row(int row, const A (&s)[NV], double (&red)[NR]) const;
-//   __device__ void finish(double (&red)[NR], double *scratch, int tile) const;
-// `row` is called exactly once per row of the tile. `finish` is called by
-// every thread of the CTA after all rows are done (it must do its own block
-// reduction; scratch is 32*8 doubles of shared memory).
-template <class T, class A, int NV, bool EXACT, class Epi>
-__device__ __forceinline__ void tile_pass(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi &epi,
-                                          TileSmem<A, NV> &sm) {
+// Kernel variants of the FAST pass (the autotuner picks one per matrix):
+//   U     32-nonzero steps per load batch (loads in flight per lane)
+//   PIPE  prefetch the next batch's indices / values while the current batch
+//         gathers and reduces
+//   MINB  resident CTAs per SM the register allocation is held to
+struct FastVariant {
+    int u, pipe, minb;
+};
+constexpr int kFastVariants = 5;
+__host__ __device__ constexpr FastVariant fast_variant(int v) {
+    return v == 0 ? FastVariant{4, 1, 12}
+                  : v == 1 ? FastVariant{8, 1, 8}
+                           : v == 2 ? FastVariant{8, 0, 12} : v == 3 ? FastVariant{16, 0, 8} : FastVariant{2, 1, 16};
+}
+
+template <class T, class A, int NV, class Epi, int U, bool PIPE, int MINB>
+__global__ void __launch_bounds__(kTileThreads, MINB)
+    tile_kernel_fast(CsrView<T> M, Gathers<T, NV> g, Epi epi) {
+    if (epi.skip()) return;
     constexpr int NR = Epi::NR;
     static_assert(NR >= 1, "epilogues declare at least one reduction slot");
-    const int tile = blockIdx.x;
-    const int tid = threadIdx.x;
-    const int r0 = M.tiles[tile], r1 = M.tiles[tile + 1];
-    const int k0 = M.ro[r0], k1 = M.ro[r1];
-    const int nz = k1 - k0, nrows = r1 - r0;
+    using Pre = typename Epi::Pre;
+    __shared__ uint32_t s_mask[kWarps][kCap / 32];
+    __shared__ uint8_t s_rows[kWarps][kTileRows];
+    __shared__ Pre s_pre[kWarps][kTileRows];
+    __shared__ double scratch[32 * 8];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt_mask = (1u << lane) - 1u;
     double red[NR];
 #pragma unroll
     for (int r = 0; r < NR; ++r) red[r] = 0.0;
+    A gs[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) gs[q] = epi.gscale(q);
+    uint32_t *mask = s_mask[warp];
+    uint8_t *lrows = s_rows[warp];
+    Pre *lpre = s_pre[warp];
 
-    if (nz > kNzTile) {
-        // One long row, streamed straight from HBM by the whole CTA.
-        A s[NV];
-        if (EXACT) {
-            if (tid == 0) {
+    for (int tile = blockIdx.x * kWarps + warp; tile < M.ntiles; tile += gridDim.x * kWarps) {
+        const int r0 = __ldg(M.tiles + tile), r1 = __ldg(M.tiles + tile + 1);
+        const int k0 = __ldg(M.tile_k + tile), k1 = __ldg(M.tile_k + tile + 1);
+        const int nz = k1 - k0, nrows = r1 - r0;
+        if (nz > kCap) {
+            // One long row, streamed by the whole warp, U loads per lane in flight.
+            const Pre pre = epi.load(r0);
+            A part[NV];
 #pragma unroll
-                for (int q = 0; q < NV; ++q) s[q] = epi.init(r0, q);
-                for (int k = k0; k < k1; ++k) {
-                    const int c = M.ci[k];
-                    const A v = static_cast<A>(M.val[k]);
+            for (int q = 0; q < NV; ++q) part[q] = A(0);
+            for (int kb = k0; kb < k1; kb += 32 * U) {
+                int c[U];
+                T v[U];
 #pragma unroll
-                    for (int q = 0; q < NV; ++q)
-                        s[q] = add_rn(s[q], mul_rn(v, mul_rn(epi.gscale(q), static_cast<A>(g.p[q][c]))));
+                for (int u = 0; u < U; ++u) {
+                    const int k = kb + 32 * u + lane;
+                    c[u] = k < k1 ? __ldg(M.ci + k) : 0;
+                    v[u] = k < k1 ? __ldg(M.val + k) : T(0);
                 }
-                epi.row(r0, s, red);
-            }
-        } else {
-            double part[NV > 0 ? NV : 1];
 #pragma unroll
-            for (int q = 0; q < NV; ++q) part[q] = 0.0;
-#pragma unroll 4
-            for (int k = k0 + tid; k < k1; k += kTileThreads) {
-                const int c = __ldg(M.ci + k);
-                const A v = static_cast<A>(__ldg(M.val + k));
+                for (int u = 0; u < U; ++u) {
+                    if (kb + 32 * u + lane < k1) {
 #pragma unroll
-                for (int q = 0; q < NV; ++q) part[q] += static_cast<double>(v * static_cast<A>(__ldg(g.p[q] + c)));
+                        for (int q = 0; q < NV; ++q)
+                            part[q] += static_cast<A>(v[u]) * (gs[q] * static_cast<A>(__ldg(g.p[q] + c[u])));
+                    }
+                }
             }
-            block_sum<NV>(part, sm.red);
-            if (tid == 0) {
+            A sum[NV];
 #pragma unroll
-                for (int q = 0; q < NV; ++q)
-                    s[q] = epi.init(r0, q) + static_cast<A>(part[q]) * epi.gscale(q);
-                epi.row(r0, s, red);
-            }
+            for (int q = 0; q < NV; ++q) sum[q] = epi.init(r0, q) + warp_sum(part[q]);
+            if (lane == 0) epi.row_pre(r0, sum, pre, red);
+            continue;
         }
-        __syncthreads();
-        epi.finish(red, sm.red, tile);
-        return;
-    }
-
-    // Multi-row tile: stage the products in shared memory.
-    if (tid == 0) sm.n_long = 0;
-    for (int i = tid; i <= nrows; i += kTileThreads) sm.rofs[i] = M.ro[r0 + i] - k0;
-    {
-        int cidx[kPer];
-        T v[kPer];
+        // The first batch's loads go out before the prologue's.
+        int cn[U];
+        T vn[U];
 #pragma unroll
-        for (int j = 0; j < kPer; ++j) {
-            const int k = tid + j * kTileThreads;
-            if (k < nz) {
-                cidx[j] = __ldg(M.ci + k0 + k);
-                v[j] = __ldg(M.val + k0 + k);
-            }
+        for (int u = 0; u < U; ++u) {
+            const int k = 32 * u + lane;
+            cn[u] = k < nz ? __ldg(M.ci + k0 + k) : 0;
+            vn[u] = k < nz ? __ldg(M.val + k0 + k) : T(0);
         }
+        // Prologue: row-end bitmask, non-empty rows in order, per-row inputs.
+        const int nwords = (nz + 31) >> 5; // kCap / 32 == 32 words: one per lane
+        if (lane < nwords) mask[lane] = 0u;
+        __syncwarp();
+        int ne_count = 0;
 #pragma unroll
-        for (int j = 0; j < kPer; ++j) {
-            const int k = tid + j * kTileThreads;
-            if (k < nz) {
+        for (int rb = 0; rb < kTileRows; rb += 32) {
+            if (rb >= nrows) break;
+            const int i = rb + lane;
+            const bool valid = i < nrows;
+            bool nonempty = false;
+            if (valid) {
+                const int a = __ldg(M.ro + r0 + i), b = __ldg(M.ro + r0 + i + 1);
+                const Pre pre = epi.load(r0 + i);
+                lpre[i] = pre;
+                nonempty = b > a;
+                if (nonempty) {
+                    const int e = b - 1 - k0;
+                    atomicOr(&mask[e >> 5], 1u << (e & 31));
+                } else {
+                    A sum[NV];
+#pragma unroll
+                    for (int q = 0; q < NV; ++q) sum[q] = epi.init(r0 + i, q);
+                    epi.row_pre(r0 + i, sum, pre, red);
+                }
+            }
+            const unsigned nem = __ballot_sync(FULL, nonempty);
+            if (nonempty) lrows[ne_count + __popc(nem & lt_mask)] = static_cast<uint8_t>(i);
+            ne_count += __popc(nem);
+        }
+        __syncwarp();
+        // Streaming steps with a segmented scan.
+        A carry[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) carry[q] = A(0);
+        int ends = 0;
+        for (int jb = 0; jb < nz; jb += 32 * U) {
+            int c[U];
+            T v[U];
+            if (!PIPE && jb > 0) {
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int k = jb + 32 * u + lane;
+                    c[u] = k < nz ? __ldg(M.ci + k0 + k) : 0;
+                    v[u] = k < nz ? __ldg(M.val + k0 + k) : T(0);
+                }
+            } else {
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    c[u] = cn[u];
+                    v[u] = vn[u];
+                }
+            }
+            A xv[NV][U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const bool in = jb + 32 * u + lane < nz;
+#pragma unroll
+                for (int q = 0; q < NV; ++q) xv[q][u] = in ? static_cast<A>(__ldg(g.p[q] + c[u])) : A(0);
+            }
+            const int jn = jb + 32 * U;
+            if (PIPE && jn < nz) {
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int k = jn + 32 * u + lane;
+                    cn[u] = k < nz ? __ldg(M.ci + k0 + k) : 0;
+                    vn[u] = k < nz ? __ldg(M.val + k0 + k) : T(0);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int pos = jb + 32 * u;
+                if (pos >= nz) break;
+                const uint32_t F = mask[pos >> 5];
+                const int seg = 32 - __clz(F & lt_mask); // first lane of this lane's segment
+                A p[NV];
+#pragma unroll
+                for (int q = 0; q < NV; ++q) p[q] = static_cast<A>(v[u]) * (gs[q] * xv[q][u]);
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+#pragma unroll
+                    for (int q = 0; q < NV; ++q) {
+                        const A t = __shfl_up_sync(FULL, p[q], d);
+                        if (lane - d >= seg) p[q] += t;
+                    }
+                }
+                if (seg == 0) {
+#pragma unroll
+                    for (int q = 0; q < NV; ++q) p[q] += carry[q];
+                }
+                if ((F >> lane) & 1u) {
+                    const int li = lrows[ends + __popc(F & lt_mask)];
+                    A sum[NV];
+#pragma unroll
+                    for (int q = 0; q < NV; ++q) sum[q] = epi.init(r0 + li, q) + p[q];
+                    epi.row_pre(r0 + li, sum, lpre[li], red);
+                }
+                const bool open = ((F >> 31) & 1u) == 0u;
 #pragma unroll
                 for (int q = 0; q < NV; ++q) {
-                    A xv = static_cast<A>(__ldg(g.p[q] + cidx[j]));
-                    if (EXACT) xv = mul_rn(epi.gscale(q), xv);
-                    sm.prod[q][k] = mul_rn(static_cast<A>(v[j]), xv);
+                    const A t = __shfl_sync(FULL, p[q], 31);
+                    carry[q] = open ? t : A(0);
                 }
+                ends += __popc(F);
             }
         }
+        __syncwarp();
     }
-    __syncthreads();
-    for (int i = tid; i < nrows; i += kTileThreads) {
-        const int a = sm.rofs[i], b = sm.rofs[i + 1];
-        if (EXACT || b - a <= kShortRow) {
-            A s[NV];
-#pragma unroll
-            for (int q = 0; q < NV; ++q) {
-                A acc = epi.init(r0 + i, q);
-                if (EXACT) {
-                    for (int k = a; k < b; ++k) acc = add_rn(acc, sm.prod[q][k]);
-                } else {
-                    A t = A(0);
-                    for (int k = a; k < b; ++k) t += sm.prod[q][k];
-                    acc = acc + t * epi.gscale(q);
-                }
-                s[q] = acc;
-            }
-            epi.row(r0 + i, s, red);
-        } else {
-            const int slot = atomicAdd(&sm.n_long, 1);
-            sm.long_list[slot] = i;
-        }
-    }
-    if (!EXACT) {
-        __syncthreads();
-        const int nl = sm.n_long;
-        const int lane = tid & 31, warp = tid >> 5;
-        for (int w = warp; w < nl; w += kTileThreads / 32) {
-            const int i = sm.long_list[w];
-            const int a = sm.rofs[i], b = sm.rofs[i + 1];
-            A s[NV];
-#pragma unroll
-            for (int q = 0; q < NV; ++q) {
-                A t = A(0);
-                for (int k = a + lane; k < b; k += 32) t += sm.prod[q][k];
-                t = warp_sum(t);
-                s[q] = epi.init(r0 + i, q) + t * epi.gscale(q);
-            }
-            if (lane == 0) epi.row(r0 + i, s, red);
-        }
-    }
-    __syncthreads();
-    epi.finish(red, sm.red, tile);
+    epi.finish(red, scratch, blockIdx.x);
 }
 
-template <class T, class A, int NV, bool EXACT, class Epi>
+// Parity kernel: one thread per row, the reference's left-to-right order.
+template <class T, class A, int NV, class Epi>
 __global__ void __launch_bounds__(kTileThreads)
-    tile_kernel(CsrView<T> M, Gathers<T, NV> g, Epi epi) {
+    tile_kernel_exact(CsrView<T> M, Gathers<T, NV> g, Epi epi) {
     if (epi.skip()) return;
-    __shared__ TileSmem<A, NV> sm;
-    tile_pass<T, A, NV, EXACT, Epi>(M, g, epi, sm);
+    constexpr int NR = Epi::NR;
+    __shared__ double scratch[32 * 8];
+    double red[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) red[r] = 0.0;
+    A gs[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) gs[q] = epi.gscale(q);
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < M.rows; r += gridDim.x * blockDim.x) {
+        const auto pre = epi.load(r);
+        A s[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) s[q] = epi.init(r, q);
+        const int b = M.ro[r], e = M.ro[r + 1];
+        for (int k = b; k < e; ++k) {
+            const int c = M.ci[k];
+            const A v = static_cast<A>(M.val[k]);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) s[q] = add_rn(s[q], mul_rn(v, mul_rn(gs[q], static_cast<A>(g.p[q][c]))));
+        }
+        epi.row_pre(r, s, pre, red);
+    }
+    epi.finish(red, scratch, blockIdx.x);
 }
 
-template <class T, class A, int NV, bool EXACT, class Epi>
-inline void launch_tiles(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi &epi, cudaStream_t s) {
-    if (M.ntiles <= 0) return;
-    tile_kernel<T, A, NV, EXACT, Epi><<<M.ntiles, kTileThreads, 0, s>>>(M, g, epi);
+template <class K>
+inline int resident_grid(K kernel) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kTileThreads, 0);
+    per = per < 1 ? 1 : (per > kMaxGridPerSM ? kMaxGridPerSM : per);
+    const int r = sms * per;
+    return r < kMaxGrid ? r : kMaxGrid;
+}
+
+template <class T, class A, int NV, class Epi, int V>
+inline int launch_fast(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi &epi, cudaStream_t s) {
+    constexpr FastVariant fv = fast_variant(V);
+    auto kernel = tile_kernel_fast<T, A, NV, Epi, fv.u, fv.pipe != 0, fv.minb>;
+    static const int resident = resident_grid(kernel);
+    const int need = (M.ntiles + kWarps - 1) / kWarps;
+    const int grid = need < resident ? (need > 0 ? need : 1) : resident;
+    kernel<<<grid, kTileThreads, 0, s>>>(M, g, epi);
     VK_LAUNCH_CHECK();
+    return grid;
 }
 
-// Epilogue base: one unused reduction slot, unit gather scale, zero start,
-// never skipped.
+// Launches the pass; returns the number of CTAs (the entries a per-CTA
+// partial-sum epilogue writes), 0 when the matrix has no rows. The grid is
+// persistent: resident CTAs per SM (occupancy calculator, at most
+// kMaxGridPerSM) times the SM count, or fewer when there is less work.
+template <class T, class A, int NV, bool EXACT, class Epi>
+inline int launch_tiles(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi &epi, cudaStream_t s) {
+    if (M.rows <= 0) return 0;
+    if (EXACT) {
+        static const int resident = resident_grid(tile_kernel_exact<T, A, NV, Epi>);
+        const int need = (M.rows + kTileThreads - 1) / kTileThreads;
+        const int grid = need < resident ? need : resident;
+        tile_kernel_exact<T, A, NV, Epi><<<grid, kTileThreads, 0, s>>>(M, g, epi);
+        VK_LAUNCH_CHECK();
+        return grid;
+    }
+    switch (M.variant) {
+    case 1: return launch_fast<T, A, NV, Epi, 1>(M, g, epi, s);
+    case 2: return launch_fast<T, A, NV, Epi, 2>(M, g, epi, s);
+    case 3: return launch_fast<T, A, NV, Epi, 3>(M, g, epi, s);
+    case 4: return launch_fast<T, A, NV, Epi, 4>(M, g, epi, s);
+    default: return launch_fast<T, A, NV, Epi, 0>(M, g, epi, s);
+    }
+}
+
+// Epilogue base: one unused reduction slot, no prefetch, unit gather scale,
+// zero start, never skipped. Derived epilogues define row() (through EpiRow)
+// or row_pre().
 template <class A>
 struct EpiBase {
     static constexpr int NR = 1;
+    struct Pre {};
+    __device__ Pre load(int) const { return Pre{}; }
     __device__ A init(int, int) const { return A(0); }
     __device__ A gscale(int) const { return A(1); }
     __device__ bool skip() const { return false; }
     __device__ void finish(double (&)[1], double *, int) const {}
+};
+
+// Adapter: epilogues without a prefetch implement row(i, s, red).
+template <class A, class Derived>
+struct EpiRow : EpiBase<A> {
+    template <int NV, int NR>
+    __device__ void row_pre(int i, const A (&s)[NV], const typename EpiBase<A>::Pre &, double (&red)[NR]) const {
+        static_cast<const Derived *>(this)->row(i, s, red);
+    }
 };
 
 // ---- setup (vk_csr.cu) ------------------------------------------------------
@@ -248,7 +414,15 @@ void transpose_pattern(const CsrPattern32 &a, CsrPattern32 &at, DevBuf<int> &per
 // dst[t] = src[perm[t]] (optionally converting the value type).
 template <class TD, class TS>
 void gather_values(const int *perm, const TS *src, TD *dst, int64_t nnz, cudaStream_t s);
+// dst[k] = (TD) src[k].
+template <class TD, class TS>
+void convert_values(const TS *src, TD *dst, int64_t n, cudaStream_t s);
 // Expands row offsets to a row index per nonzero.
 void expand_rows(const CsrPattern32 &p, int *rowidx, cudaStream_t s);
+// Autotuner: times every FAST kernel variant on this matrix (a plain product
+// into scratch vectors, a few launches each) and stores the fastest in
+// p.variant. Matrices below `min_nnz` keep variant 0.
+template <class T>
+void autotune_pattern(CsrPattern32 &p, const T *val, cudaStream_t s, int64_t min_nnz = 200000);
 
 } // namespace vk

@@ -166,15 +166,17 @@ std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s) {
     dm->offset = p.objective_offset;
     static const int64_t zero = 0;
     upload_pattern(m, n, m > 0 ? p.A.row_offsets : &zero, p.A.col_indices, dm->a, s);
-    dm->a_val.reset(dm->nnz > 0 ? dm->nnz : 1);
+    dm->a_val.reset(padded(dm->nnz));
     if (dm->nnz > 0)
         VK_CUDA(cudaMemcpyAsync(dm->a_val.get(), p.A.values, dm->nnz * sizeof(double), cudaMemcpyHostToDevice, s));
     transpose_pattern(dm->a, dm->at, dm->perm, s);
-    dm->at_val.reset(dm->nnz > 0 ? dm->nnz : 1);
+    dm->at_val.reset(padded(dm->nnz));
     gather_values<double, double>(dm->perm.get(), dm->a_val.get(), dm->at_val.get(), dm->nnz, s);
+    autotune_pattern<double>(dm->a, dm->a_val.get(), s);
+    autotune_pattern<double>(dm->at, dm->at_val.get(), s);
     if (dm->qp) {
         upload_pattern(n, n, p.Q.row_offsets, p.Q.col_indices, dm->q, s);
-        dm->q_val.reset(dm->q_nnz);
+        dm->q_val.reset(padded(dm->q_nnz));
         VK_CUDA(cudaMemcpyAsync(dm->q_val.get(), p.Q.values, dm->q_nnz * sizeof(double), cudaMemcpyHostToDevice, s));
         dm->h_qro.assign(p.Q.row_offsets, p.Q.row_offsets + n + 1);
         dm->h_qci.assign(p.Q.col_indices, p.Q.col_indices + dm->q_nnz);
@@ -236,7 +238,7 @@ namespace {
 constexpr int kPostRowSums = 4; // rp2, b2, dobj_rows, viol2
 constexpr int kPostColSums = 6; // box2, c2, rd2, dobj_cols, pobj, quad
 
-struct PostRowEpi : EpiBase<double> {
+struct PostRowEpi : EpiRow<double, PostRowEpi> {
     static constexpr int NR = 6; // [0] pr max [1] comp max, then sums
     const double *rl, *ru, *yo;
     double *ld, *ud;
@@ -281,7 +283,7 @@ struct PostRowEpi : EpiBase<double> {
     }
 };
 
-struct PostColEpi : EpiBase<double> {
+struct PostColEpi : EpiRow<double, PostColEpi> {
     static constexpr int NR = 10; // [0] stat max [1] comp max [2] box max [3] nonfinite, then sums
     const double *xo, *lo, *hi, *c, *qc;
     double atol;
@@ -348,7 +350,7 @@ struct PostColEpiInit : PostColEpi {
     __device__ double init(int j, int) const { return init_value(j); }
 };
 
-struct QcEpi : EpiBase<double> {
+struct QcEpi : EpiRow<double, QcEpi> {
     const double *c;
     double *out;
     __device__ double init(int j, int) const { return c[j]; }
@@ -362,6 +364,7 @@ struct QcEpi : EpiBase<double> {
 // ---------------------------------------------------------------------------
 Solver::Solver(const vk_problem &p, const vk_options &o) : opts_(o) {
     VK_CUDA(cudaSetDevice(o.device));
+    device_error_flag(); // allocated here, never inside a graph capture
     VK_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     dm_ = upload_model(p, stream_);
     engine_ = o.algorithm == VK_ALGO_HALPERN ? make_halpern_engine(*dm_, o, stream_)
@@ -432,8 +435,8 @@ void Solver::solve(const double *warm, const double *lo_ovr, const double *hi_ov
     VK_CUDA(cudaMemsetAsync(post.get(), 0, sizeof(PostOut), s));
     DevBuf<double> ld(r->row_lower_dual && m ? m : 0), ud(r->row_upper_dual && m ? m : 0);
     DevBuf<double> vld(r->var_lower_dual ? n : 0), vud(r->var_upper_dual ? n : 0);
-    DevBuf<double> prow(static_cast<size_t>(std::max(dm.a.ntiles, 1)) * kPostRowSums);
-    DevBuf<double> pcol(static_cast<size_t>(std::max(dm.at.ntiles, 1)) * kPostColSums);
+    DevBuf<double> prow(static_cast<size_t>(kMaxGrid) * kPostRowSums);
+    DevBuf<double> pcol(static_cast<size_t>(kMaxGrid) * kPostColSums);
     DevBuf<double> sums(kPostRowSums + kPostColSums);
     VK_CUDA(cudaMemsetAsync(sums.get(), 0, sums.bytes(), s));
     if (m > 0) {
@@ -445,11 +448,10 @@ void Solver::solve(const double *warm, const double *lo_ovr, const double *hi_ov
         e.ud = ud.get();
         e.out = post.get();
         e.partials = prow.get();
-        if (exact)
-            launch_tiles<double, double, 1, true>(view(dm.a, dm.a_val.get()), Gathers<double, 1>{{xo.get()}}, e, s);
-        else
-            launch_tiles<double, double, 1, false>(view(dm.a, dm.a_val.get()), Gathers<double, 1>{{xo.get()}}, e, s);
-        reduce_partials(prow.get(), dm.a.ntiles, kPostRowSums, sums.get(), s);
+        const int grid =
+            exact ? launch_tiles<double, double, 1, true>(view(dm.a, dm.a_val.get()), Gathers<double, 1>{{xo.get()}}, e, s)
+                  : launch_tiles<double, double, 1, false>(view(dm.a, dm.a_val.get()), Gathers<double, 1>{{xo.get()}}, e, s);
+        reduce_partials(prow.get(), grid, kPostRowSums, sums.get(), s);
     }
     DevBuf<double> qc(dm.qp ? n : 0);
     if (dm.qp) {
@@ -474,11 +476,10 @@ void Solver::solve(const double *warm, const double *lo_ovr, const double *hi_ov
         e.out = post.get();
         e.partials = pcol.get();
         const double *ygather = m > 0 ? yo.get() : xo.get(); // never read when A has no entries
-        if (exact)
-            launch_tiles<double, double, 1, true>(view(dm.at, dm.at_val.get()), Gathers<double, 1>{{ygather}}, e, s);
-        else
-            launch_tiles<double, double, 1, false>(view(dm.at, dm.at_val.get()), Gathers<double, 1>{{ygather}}, e, s);
-        reduce_partials(pcol.get(), dm.at.ntiles, kPostColSums, sums.get() + kPostRowSums, s);
+        const int grid =
+            exact ? launch_tiles<double, double, 1, true>(view(dm.at, dm.at_val.get()), Gathers<double, 1>{{ygather}}, e, s)
+                  : launch_tiles<double, double, 1, false>(view(dm.at, dm.at_val.get()), Gathers<double, 1>{{ygather}}, e, s);
+        reduce_partials(pcol.get(), grid, kPostColSums, sums.get() + kPostRowSums, s);
     }
     PostOut hp;
     double hs[kPostRowSums + kPostColSums];

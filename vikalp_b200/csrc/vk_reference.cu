@@ -109,14 +109,17 @@ struct RefColEpi : EpiBase<double> {
     RefCtl *ctl;
     double *aty;
     const double *x, *c, *l, *u, *qx;
+    struct Pre {
+        double x, c, l, u, qx;
+    };
     __device__ bool skip() const { return ctl->done != 0; }
-    __device__ void row(int j, const double (&s)[1], double (&red)[1]) const {
+    __device__ Pre load(int j) const { return Pre{x[j], c[j], l[j], u[j], QP ? qx[j] : 0.0}; }
+    __device__ void row_pre(int j, const double (&s)[1], const Pre &p, double (&red)[1]) const {
         aty[j] = s[0];
         if (ctl->iter >= 1) {
-            const double g = QP ? __dadd_rn(s[0], __dadd_rn(c[j], qx[j])) : __dadd_rn(s[0], c[j]);
-            const double xj = x[j];
-            const double px = clampbox(__dadd_rn(-g, xj), l[j], u[j]);
-            red[0] = smax(red[0], fabs(__dadd_rn(-px, xj)));
+            const double g = QP ? __dadd_rn(s[0], __dadd_rn(p.c, p.qx)) : __dadd_rn(s[0], p.c);
+            const double px = clampbox(__dadd_rn(-g, p.x), p.l, p.u);
+            red[0] = smax(red[0], fabs(__dadd_rn(-px, p.x)));
         }
     }
     __device__ void finish(double (&red)[1], double *scratch, int) const {
@@ -129,26 +132,29 @@ struct RefRowEpi : EpiBase<double> {
     RefCtl *ctl;
     double *y;
     const double *rl, *ru;
+    struct Pre {
+        double y, rl, ru;
+    };
     __device__ bool skip() const { return ctl->done != 0; }
-    __device__ void row(int i, const double (&s)[2], double (&red)[1]) const {
+    __device__ Pre load(int i) const { return Pre{y[i], rl[i], ru[i]}; }
+    __device__ void row_pre(int i, const double (&s)[2], const Pre &p, double (&red)[1]) const {
         const double sigma = ctl->sigma, inv = ctl->inv_sigma;
-        const double yarg = __dadd_rn(__dmul_rn(sigma, s[0]), y[i]);
-        const double lo = rl[i], hi = ru[i];
-        const double yp = clampbox(__dmul_rn(inv, yarg), lo, hi);
+        const double yarg = __dadd_rn(__dmul_rn(sigma, s[0]), p.y);
+        const double yp = clampbox(__dmul_rn(inv, yarg), p.rl, p.ru);
         y[i] = __dadd_rn(__dmul_rn(-sigma, yp), yarg);
-        const double pax = clampbox(s[1], lo, hi);
+        const double pax = clampbox(s[1], p.rl, p.ru);
         red[0] = smax(red[0], fabs(__dadd_rn(pax, -s[1])));
     }
-    __device__ void finish(double (&red)[1], double *scratch, int tile) const {
+    __device__ void finish(double (&red)[1], double *scratch, int block) const {
         const double v = block_max_nonneg(red[0], scratch);
         if (threadIdx.x == 0) {
             atomic_max_nonneg(&ctl->rp, v);
-            if (tile == 0) atomicAdd(reinterpret_cast<unsigned long long *>(&ctl->iter), 1ull);
+            if (block == 0) atomicAdd(reinterpret_cast<unsigned long long *>(&ctl->iter), 1ull);
         }
     }
 };
 
-struct StoreEpi : EpiBase<double> {
+struct StoreEpi : EpiRow<double, StoreEpi> {
     RefCtl *ctl;
     double *out;
     __device__ bool skip() const { return ctl && ctl->done != 0; }
@@ -225,8 +231,8 @@ public:
         const int m = dm.m, n = dm.n;
         rs_.reset(m > 0 ? m : 1);
         cs_.reset(n);
-        ka_.reset(dm.nnz > 0 ? dm.nnz : 1);
-        kat_.reset(dm.nnz > 0 ? dm.nnz : 1);
+        ka_.reset(padded(dm.nnz));
+        kat_.reset(padded(dm.nnz));
         sc_.reset(n);
         srl_.reset(m > 0 ? m : 1);
         sru_.reset(m > 0 ? m : 1);
@@ -257,7 +263,7 @@ public:
         abs_rowsum_max_kernel<<<ceil_div(n, 256), 256, 0, s>>>(dm.at.ro.get(), kat_.get(), n, mx.get() + 1);
         VK_LAUNCH_CHECK();
         if (dm.qp) {
-            kq_.reset(dm.q_nnz);
+            kq_.reset(padded(dm.q_nnz));
             scale_values_kernel<<<ceil_div(int64_t(n) * 32, 256), 256, 0, s>>>(
                 dm.q.ro.get(), dm.q.ci.get(), dm.q_val.get(), cs_.get(), cs_.get(), n, false, kq_.get());
             abs_rowsum_max_kernel<<<ceil_div(n, 256), 256, 0, s>>>(dm.q.ro.get(), kq_.get(), n, mx.get() + 2);
@@ -321,6 +327,7 @@ public:
             VK_CUDA(cudaGraphLaunch(graph_exec_, s_));
             VK_CUDA(cudaMemcpyAsync(hctl_.get(), ctl_.get(), sizeof(RefCtl), cudaMemcpyDeviceToHost, s_));
             VK_CUDA(cudaStreamSynchronize(s_));
+            check_device_error(s_);
             if (hctl_[0].done) break;
         }
         VK_CUDA(cudaEventRecord(e1, s_));
