@@ -1,0 +1,323 @@
+#!/usr/bin/env python
+"""Benchmark of the PDHG LP hot path on B200.
+
+Workload: the large seeded LP (m=1,000,000, n=2,000,000, ~21.1M nonzeros,
+Zipf(1.5) column degrees clamped at 2000 and thinned, values +-10^U[-3,3];
+vikalp_b200.synthetic.workload_large_lp). Synthetic data: no dataset exists
+for this path.
+
+A step is one check interval of 64 PDHG iterations over that LP. `value` is
+PDHG iterations per second of the reference scheme (pdhg.cpp:87-151, the
+same algorithm the reference arm runs on the CPU) on resident device data,
+timed with CUDA events on the solver's stream between a barrier + synchronize
+on both sides; whole-job = the sum over ranks (each rank solves its own copy:
+replicas, no collective on the path). The same line carries:
+  e2e            the same metric through the C ABI from host arrays (model
+                 upload, device setup, iterations, results copied back)
+  halpern        iterations/s of the restarted Halpern scheme, fp64 and mixed
+  time_to_tol    time and iterations to 1e-6 relative KKT (small LP and, with
+                 --ttt, the large LP), fp64 vs mixed
+  spmv           GB/s of the sparse product kernel, A x and A'y, fp64 / fp32
+  roofline       the sparse-pass kernel against measured HBM bandwidth
+  cpu_baseline   the reference's CPU implementation on this host
+`python bench.py --impl reference` times the reference's own CPU PDHG
+iteration (oracle/_ref, compiled from the reference sources) on the same LP.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CHUNK = 64  # iterations per step (one device-side check interval)
+METRIC = "PDHG LP iterations/s (reference scheme; m=1e6 n=2e6 nnz=21.1M); time to 1e-6 rel KKT and SpMV GB/s in-line"
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([s.strip() for s in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if len(s) > 8 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) > 8 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples if len(s) > 8 for i in range(4)
+                          if s[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup(n_gpus):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local, dist
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def allmax(dist, v, local):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the sparse-pass kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "spmv_large_lp.md")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+def spmv_figures(inst, torch, stream):
+    """GB/s of the sparse product kernel (A x and A'y, fp64 and fp32), live CUDA events."""
+    import vikalp_b200 as vk
+    out = {}
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for prec, dt in (("fp64", torch.float64), ("fp32", torch.float32)):
+        A = vk.SpMat(inst.row_offsets, inst.col_idx, inst.values, inst.m, inst.n,
+                     "fp64" if prec == "fp64" else "mixed")
+        for tr in (False, True):
+            xl, yl = (inst.m, inst.n) if tr else (inst.n, inst.m)
+            x = torch.rand(xl, dtype=dt, device="cuda")
+            y = torch.zeros(yl, dtype=dt, device="cuda")
+            for _ in range(3):
+                A.apply(x.data_ptr(), y.data_ptr(), tr, stream.cuda_stream)
+            ts = []
+            for _ in range(10):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                A.apply(x.data_ptr(), y.data_ptr(), tr, stream.cuda_stream)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            ms = statistics.median(ts)
+            out[f"{prec}_{'At_y' if tr else 'A_x'}"] = {
+                "ms": round(ms, 4), "bytes": A.bytes(tr), "gbs": round(A.bytes(tr) / ms / 1e6, 1),
+                "variant": A.variant(tr)}
+        A.close()
+    return out
+
+
+def time_to_tolerance(inst, label, limit):
+    import vikalp_b200 as vk
+    res = {}
+    for prec in ("fp64", "mixed"):
+        with vk.Pdhg(inst, algorithm="halpern", precision=prec, iteration_limit=limit,
+                     relative_tolerance=1e-6) as h:
+            r = h.solve(duals=False)
+        res[prec] = {"status": r["status"], "iterations": r["iterations"], "fp32_iterations": r["fp32_iterations"],
+                     "iterate_s": round(r["iterate_seconds"], 4), "solve_s": round(r["solve_seconds"], 4),
+                     "rel_kkt": max(r["rel_primal"], r["rel_dual"], r["rel_gap"]), "objective": r["objective"]}
+    f, mx = res["fp64"], res["mixed"]
+    if f["status"] == "Optimal" and mx["status"] == "Optimal":
+        res["mixed_speedup_vs_fp64"] = round(f["iterate_s"] / mx["iterate_s"], 3)
+    res["workload"] = label
+    return res
+
+
+def reference_cpu_rate(inst, budget_s):
+    """Iterations/s of the reference's own CPU PDHG iteration (pdhg.cpp:92-130 call
+    sequence through its CPU ExecutionBackend), a bounded sample sized by budget_s."""
+    from oracle.oracle import Reference
+    from oracle.oracle import Oracle
+    ref = Reference()
+    step = 0.99 / max(1.0, Oracle().operator_bound(inst.row_offsets, inst.col_idx, inst.values, inst.n))
+    secs1, _, _ = ref.pdhg_replay(inst, step, 1)
+    iters = max(1, min(200, int(budget_s / max(secs1, 1e-6))))
+    secs, _, _ = ref.pdhg_replay(inst, step, iters)
+    return iters / secs, iters, secs
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--ttt", action="store_true", help="also time the large LP to 1e-6 relative KKT")
+    ap.add_argument("--no-extras", action="store_true")
+    args = ap.parse_args()
+    K, W = max(1, args.steps), max(3, args.warmup)
+    ws, rank, local, dist = dist_setup(args.gpus)
+    from vikalp_b200 import synthetic
+    config = {"workload": "lp m=1,000,000 n=2,000,000 nnz~21.1M (Zipf 1.5 column degrees, |a| in 1e-3..1e3)",
+              "step": f"{CHUNK} PDHG iterations", "inputs_vs_l2": "inputs larger than L2 (~0.6 GB of matrix per iteration)",
+              "parallelism": f"replicas x{ws}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        inst = synthetic.workload_large_lp(seed=12345)
+        cores = 1
+        rate, iters, secs = reference_cpu_rate(inst, budget_s=min(120.0, 6.0 * (K + W)))
+        line = {"metric": METRIC, "value": round(rate, 4), "unit": "iter/s", "n_gpus": args.gpus, "steps": iters,
+                "warmup": 1, "ms_per_step": round(secs / iters * CHUNK * 1e3, 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": dict(config, parallelism="1 CPU core (the reference backend is single-threaded)"),
+                "cpu_baseline": {"value": round(rate, 4), "unit": "iter/s", "cores": cores, "kind": "reference",
+                                 "sample": f"{iters} iterations of the pdhg.cpp:92-130 ExecutionBackend call "
+                                           f"sequence on the large LP (its own setup is O(n*nnz) and cannot run)"},
+                "e2e": {"value": round(rate, 4), "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+
+    import vikalp_b200 as vk
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    inst = synthetic.workload_large_lp(seed=12345 + rank)
+    # ---- value: resident data, reference scheme -------------------------------
+    h = vk.Pdhg(inst, algorithm="reference", check_every=CHUNK)
+    # warm-up: W steps
+    barrier(dist)
+    torch.cuda.synchronize()
+    _ = solve_with_limit(h, W * CHUNK)
+    barrier(dist)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        barrier(dist)
+        torch.cuda.synchronize()
+        r = solve_with_limit(h, K * CHUNK)
+        torch.cuda.synchronize()
+        barrier(dist)
+    t_dev = allmax(dist, r["iterate_seconds"], local)
+    iters = r["iterations"]
+    value = ws * iters / t_dev
+    ms_per_step = t_dev / (iters / CHUNK) * 1e3
+    launches = r["kernel_launches"]
+    h.close()
+    # ---- e2e: through the C ABI from host arrays ---------------------------------
+    barrier(dist)
+    t0 = time.perf_counter()
+    r2 = vk.solve(inst, algorithm="reference", iteration_limit=K * CHUNK, primal_tolerance=0.0, dual_tolerance=0.0)
+    torch.cuda.synchronize()
+    t_e2e = allmax(dist, time.perf_counter() - t0, local)
+    h2d = (inst.row_offsets.nbytes + inst.col_idx.nbytes + inst.values.nbytes + inst.c.nbytes +
+           inst.var_lower.nbytes + inst.var_upper.nbytes + inst.row_lower.nbytes + inst.row_upper.nbytes)
+    d2h = 8 * (3 * inst.n + 3 * inst.m)  # x, variable duals; y, row duals
+    steps_e2e = max(1, r2["iterations"] // CHUNK)
+    e2e = {"value": round(ws * r2["iterations"] / t_e2e, 3), "unit": "iter/s",
+           "h2d_bytes_per_step": int(h2d / steps_e2e), "d2h_bytes_per_step": int(d2h / steps_e2e),
+           "seconds": round(t_e2e, 3), "note": "create (upload + device setup) + solve + results, pageable host arrays"}
+    line = {"metric": METRIC, "value": round(value, 3), "unit": "iter/s", "n_gpus": ws, "steps": iters // CHUNK,
+            "warmup": W, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+            "clocks": clk.summary(), "e2e": e2e, "gpu_launches": int(launches)}
+    if rank == 0 and not args.no_extras:
+        peak, peak_kind = measured_peaks()
+        sp = spmv_figures(inst, torch, stream)
+        dom = sp["fp64_A_x"]
+        achieved = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9
+        line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                            "frac": round(achieved / peak, 4), "traffic": profile_traffic(),
+                            "kernel": "tile_kernel_fast (sparse pass, A x, fp64)",
+                            "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                            "algorithmic_bytes": dom["bytes"], "ms": dom["ms"]}
+        line["spmv"] = sp
+        # Halpern scheme iteration rate (fp64 and mixed)
+        hal = {}
+        for prec in ("fp64", "mixed"):
+            with vk.Pdhg(inst, algorithm="halpern", precision=prec, check_every=CHUNK) as hh:
+                rr = solve_with_limit(hh, 10 * CHUNK, rel_tol=0.0)
+            hal[prec] = {"iter_per_s": round(rr["iterations"] / rr["iterate_seconds"], 2),
+                         "iterations": rr["iterations"]}
+        line["halpern"] = hal
+        small = synthetic.workload_small_lp()
+        ttt = {"small_lp": time_to_tolerance(small, "lp m=2000 n=5000 nnz=40000", 400000)}
+        if args.ttt:
+            ttt["large_lp"] = time_to_tolerance(inst, "large lp", 2_000_000)
+        line["time_to_tol"] = ttt
+        if ws == 1:
+            rate, n_it, secs = reference_cpu_rate(inst, budget_s=20.0)
+            line["cpu_baseline"] = {"value": round(rate, 4), "unit": "iter/s", "cores": 1, "kind": "reference",
+                                    "sample": f"{n_it} iterations of the reference's pdhg.cpp:92-130 call sequence "
+                                              f"(its CPU ExecutionBackend) on the large LP, {secs:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def solve_with_limit(h, limit, rel_tol=0.0):
+    """One vk_pdhg_solve with a fixed iteration budget (tolerances 0: runs the full budget)."""
+    return h.solve(duals=False, iteration_limit=limit, primal_tolerance=0.0, dual_tolerance=0.0,
+                   relative_tolerance=rel_tol)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -123,6 +123,7 @@ typedef struct {
     double solve_seconds;
     double iterate_seconds; /* device time of the iteration loop alone */
     int64_t fp32_iterations; /* MIXED: iterations done in FP32 */
+    int64_t kernel_launches; /* kernels this library launched in the iteration loop */
     char message[256];
 } vk_result;
 
@@ -147,6 +148,15 @@ int vk_pdhg_create(const vk_problem *problem, const vk_options *opts, vk_pdhg **
  * reference returns a SolveResult rather than throwing. */
 int vk_pdhg_solve(vk_pdhg *h, const double *warm_start, const double *var_lower_override,
                   const double *var_upper_override, vk_result *result);
+
+/* Changes the per-solve options of a handle for its next solves: the limits
+ * and tolerances (iteration_limit, time_limit_seconds, primal_tolerance,
+ * dual_tolerance, relative_tolerance, verbose), as the reference passes
+ * SolverOptions to every RelaxationOracle::solve call
+ * (RelaxationOracle.hpp:17-22). Every other field must equal the one the
+ * handle was created with (VK_ERR_INVALID otherwise); invalid limits are
+ * rejected with the reference's message (continuous_common.hpp:50-56). */
+int vk_pdhg_set_options(vk_pdhg *h, const vk_options *opts);
 
 void vk_pdhg_destroy(vk_pdhg *h);
 

@@ -1,0 +1,165 @@
+"""NumPy restatement of the restarted reflected-Halpern PDHG -- TEST INFRASTRUCTURE ONLY.
+
+This is the checker for the library's VK_ALGO_HALPERN engine (no reference
+counterpart: the reference runs the fixed every-50-iterations scheme of
+pdhg.cpp:133-145). It follows the same definitions, float64 throughout:
+
+* scaling: 10 Ruiz infinity-norm passes then one Pock-Chambolle (alpha=1) pass
+  (R, D), K = R A D, c^ = D c, variable bounds / D, row bounds * R;
+* eta = 0.99 / sigma_max(K) (power iteration), omega_0 = |c^| / |b^|;
+* the PDHG step with the reference's sign convention for y and the reflected
+  Halpern update with lambda = (k+1)/(k+2);
+* every `check_every` iterations: relative KKT of (x^, y^) in original units,
+  stop at `tol`, restart rule on the fixed-point residual, primal weight
+  update on restart.
+
+Used by tests/ and the bench's CPU baseline only.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+
+
+def _csr(inst):
+    return sp.csr_matrix((inst.values, inst.col_idx, inst.row_offsets), shape=(inst.m, inst.n))
+
+
+def scaling(A: sp.csr_matrix, passes: int = 10):
+    m, n = A.shape
+    r = np.ones(m)
+    d = np.ones(n)
+    absA = abs(A)
+    for p in range(passes + 1):
+        K = sp.diags(r) @ absA @ sp.diags(d)
+        if p < passes:
+            rn = np.asarray(K.max(axis=1).todense()).ravel() if m else np.zeros(0)
+            cn = np.asarray(K.max(axis=0).todense()).ravel()
+        else:
+            rn = np.asarray(K.sum(axis=1)).ravel()
+            cn = np.asarray(K.sum(axis=0)).ravel()
+        r = np.where(rn > 0, r / np.sqrt(np.where(rn > 0, rn, 1)), r)
+        d = np.where(cn > 0, d / np.sqrt(np.where(cn > 0, cn, 1)), d)
+    return r, d
+
+
+def sigma_max(K: sp.csr_matrix, iters: int = 200) -> float:
+    n = K.shape[1]
+    i = np.arange(n, dtype=np.uint64)
+    h = (i * np.uint64(2654435761) + np.uint64(12345)) & np.uint64(0xFFFFFFFF)
+    h ^= h >> np.uint64(13)
+    h = (h * np.uint64(2246822519)) & np.uint64(0xFFFFFFFF)
+    h ^= h >> np.uint64(16)
+    v = 0.5 + (h & np.uint64(0xFFFF)).astype(np.float64) / 65536.0
+    v /= np.linalg.norm(v)
+    prev = 0.0
+    for it in range(iters):
+        z = K.T @ (K @ v)
+        nz = np.linalg.norm(z)
+        est = np.sqrt(nz)
+        v = z / nz if nz > 0 else z
+        if it > 10 and abs(est - prev) <= 1e-6 * est:
+            return est
+        prev = est
+    return prev
+
+
+def rel_kkt(inst, x, y, lower=None, upper=None):
+    """Relative KKT of (x, y) in original units (same definition as the C oracle)."""
+    A = _csr(inst)
+    lo = inst.var_lower if lower is None else lower
+    hi = inst.var_upper if upper is None else upper
+    ax = A @ x
+    rl, ru = inst.row_lower, inst.row_upper
+    rp = np.linalg.norm(ax - np.clip(ax, rl, ru)) + np.linalg.norm(x - np.clip(x, lo, hi))
+    b = np.maximum(np.where(np.isfinite(rl), np.abs(rl), 0), np.where(np.isfinite(ru), np.abs(ru), 0))
+    lam = inst.c + A.T @ y
+    yl, yu = np.maximum(0, -y), np.maximum(0, y)
+    vl, vu = np.maximum(0, lam), np.maximum(0, -lam)
+    viol = np.sum(np.where((yl > 0) & ~np.isfinite(rl), yl, 0) ** 2) + np.sum(np.where((yu > 0) & ~np.isfinite(ru), yu, 0) ** 2)
+    rd2 = np.sum(np.where((vl > 0) & ~np.isfinite(lo), vl, 0) ** 2) + np.sum(np.where((vu > 0) & ~np.isfinite(hi), vu, 0) ** 2)
+    fin = lambda v, w: np.where((w > 0) & np.isfinite(v), v * w, 0.0)  # noqa: E731
+    dobj = np.sum(fin(rl, yl)) - np.sum(fin(ru, yu)) + np.sum(fin(lo, vl)) - np.sum(fin(hi, vu))
+    pobj = inst.c @ x
+    return dict(rel_primal=rp / (1 + np.linalg.norm(b)), rel_dual=np.sqrt(rd2 + viol) / (1 + np.linalg.norm(inst.c)),
+                rel_gap=abs(pobj - dobj) / (1 + abs(pobj) + abs(dobj)), primal_objective=pobj, dual_objective=dobj)
+
+
+def solve(inst, tol=1e-6, iteration_limit=100000, check_every=64, rho=1.0, warm=None, lower=None, upper=None,
+          trace=False):
+    A = _csr(inst)
+    m, n = A.shape
+    lo0 = inst.var_lower if lower is None else lower
+    hi0 = inst.var_upper if upper is None else upper
+    r, d = scaling(A)
+    K = (sp.diags(r) @ A @ sp.diags(d)).tocsr()
+    KT = K.T.tocsr()
+    c = inst.c * d
+    with np.errstate(invalid="ignore", divide="ignore"):
+        lo = np.where(np.isfinite(lo0), lo0 / d, lo0)
+        hi = np.where(np.isfinite(hi0), hi0 / d, hi0)
+        rl = np.where(np.isfinite(inst.row_lower), inst.row_lower * r, inst.row_lower)
+        ru = np.where(np.isfinite(inst.row_upper), inst.row_upper * r, inst.row_upper)
+    b_orig = np.maximum(np.where(np.isfinite(inst.row_lower), np.abs(inst.row_lower), 0),
+                        np.where(np.isfinite(inst.row_upper), np.abs(inst.row_upper), 0))
+    bnorm, cnorm = np.linalg.norm(b_orig), np.linalg.norm(inst.c)
+    cs2, bs2 = np.sum(c * c), np.sum((b_orig * r) ** 2)
+    omega = np.sqrt(cs2) / np.sqrt(bs2) if (cs2 > 1e-20 and bs2 > 1e-20) else 1.0
+    smax = sigma_max(K) if K.nnz else 0.0
+    eta = 0.99 / smax if smax > 0 else 1.0
+    tau, sigma = eta / omega, eta * omega
+    x = np.clip(np.zeros(n) if warm is None else warm / d, lo, hi)
+    y = np.zeros(m)
+    x0, y0 = x.copy(), y.copy()
+    k_base, total, restarts = 0, 0, 0
+    r_restart, r_prev = -1.0, np.inf
+    status, hist = "IterationLimit", []
+    xh = yh = None
+    while True:
+        for it in range(check_every):
+            lam = (k_base + it + 1.0) / (k_base + it + 2.0)
+            xh = np.clip(x - tau * (c + KT @ y), lo, hi)
+            xb = 2 * xh - x
+            xn = lam * ((1 + rho) * xh - rho * x) + (1 - lam) * x0
+            v = y + sigma * (K @ xb)
+            yh = v - np.clip(v, sigma * rl, sigma * ru)
+            yn = lam * ((1 + rho) * yh - rho * y) + (1 - lam) * y0
+            if it == check_every - 1:
+                dx2, dx0 = np.sum((xh - x) ** 2), np.sum((xh - x0) ** 2)
+                dy2, dy0 = np.sum((yh - y) ** 2), np.sum((yh - y0) ** 2)
+            x, y = xn, yn
+        total += check_every
+        kk = rel_kkt(inst, xh * d, yh * r, lo0, hi0)
+        kkt = max(kk["rel_primal"], kk["rel_dual"], kk["rel_gap"])
+        if trace:
+            hist.append((total, kkt, restarts, omega))
+        if kkt <= tol:
+            status = "Optimal"
+            break
+        if total >= iteration_limit:
+            break
+        rr = np.sqrt(omega * dx2 + dy2 / omega)
+        k = k_base + check_every
+        restart = False
+        if r_restart < 0:
+            r_restart = rr
+        else:
+            restart = rr <= 0.2 * r_restart or (rr <= 0.8 * r_restart and rr > r_prev) or k >= 0.36 * total
+        r_prev = rr
+        if restart:
+            mx, my = np.sqrt(dx0), np.sqrt(dy0)
+            if mx > 1e-10 and my > 1e-10:
+                omega = np.exp(0.5 * np.log(my / mx) + 0.5 * np.log(omega))
+            tau, sigma = eta / omega, eta * omega
+            k_base = 0
+            restarts += 1
+            r_restart = rr
+            x, x0, y, y0 = xh.copy(), xh.copy(), yh.copy(), yh.copy()
+        else:
+            k_base = k
+    out = dict(status=status, iterations=total, restarts=restarts, x=xh * d, y=yh * r, kkt=kkt, omega=omega, eta=eta)
+    out.update(kk)
+    if trace:
+        out["trace"] = hist
+    return out

@@ -70,7 +70,7 @@ class Result(C.Structure):
                 ("complementarity_residual", C.c_double), ("rel_primal", C.c_double),
                 ("rel_dual", C.c_double), ("rel_gap", C.c_double), ("last_metric", C.c_double),
                 ("solve_seconds", C.c_double), ("iterate_seconds", C.c_double),
-                ("fp32_iterations", C.c_int64), ("message", C.c_char * 256)]
+                ("fp32_iterations", C.c_int64), ("kernel_launches", C.c_int64), ("message", C.c_char * 256)]
 
 
 # Every symbol include/vikalp_b200.h declares, with its ctypes signature.
@@ -80,6 +80,7 @@ _SIGNATURES = {
     "vk_version": (C.c_char_p, []),
     "vk_pdhg_create": (C.c_int, [C.POINTER(Problem), C.POINTER(Options), C.POINTER(C.c_void_p)]),
     "vk_pdhg_solve": (C.c_int, [C.c_void_p, _f64p, _f64p, _f64p, C.POINTER(Result)]),
+    "vk_pdhg_set_options": (C.c_int, [C.c_void_p, C.POINTER(Options)]),
     "vk_pdhg_destroy": (None, [C.c_void_p]),
     "vk_csr_transpose": (C.c_int, [C.POINTER(Csr), _i64p, _i64p, _f64p, _i64p]),
     "vk_spmv": (C.c_int, [C.POINTER(Csr), C.c_double, _f64p, C.c_double, _f64p, C.c_int, C.c_int]),
@@ -183,7 +184,18 @@ class Pdhg:
         self._h = h
         self._keep.clear()
 
-    def solve(self, warm=None, lower=None, upper=None, duals: bool = True) -> dict:
+    def set_options(self, **limits):
+        """Per-solve limits / tolerances (vk_pdhg_set_options)."""
+        o = Options()
+        C.pointer(o)[0] = self.opts
+        for k, v in limits.items():
+            setattr(o, k, v)
+        _check(lib().vk_pdhg_set_options(self._h, C.byref(o)))
+        self.opts = o
+
+    def solve(self, warm=None, lower=None, upper=None, duals: bool = True, **limits) -> dict:
+        if limits:
+            self.set_options(**limits)
         keep = _Keep()
         m, n = self.m, self.n
         out = {"x": np.zeros(n), "y": np.zeros(m)}
@@ -200,7 +212,8 @@ class Pdhg:
                    complementarity_residual=r.complementarity_residual, rel_primal=r.rel_primal,
                    rel_dual=r.rel_dual, rel_gap=r.rel_gap, last_metric=r.last_metric,
                    solve_seconds=r.solve_seconds, iterate_seconds=r.iterate_seconds,
-                   fp32_iterations=r.fp32_iterations, message=r.message.decode())
+                   fp32_iterations=r.fp32_iterations, kernel_launches=r.kernel_launches,
+                   message=r.message.decode())
         return out
 
     def close(self):

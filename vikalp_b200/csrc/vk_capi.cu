@@ -156,6 +156,15 @@ int vk_pdhg_solve(vk_pdhg *h, const double *warm, const double *lo, const double
     });
 }
 
+int vk_pdhg_set_options(vk_pdhg *h, const vk_options *opts) {
+    return guarded([&] {
+        if (!h || !opts) return set_error(VK_ERR_INVALID, "null argument");
+        const std::string msg = h->solver->set_options(*opts);
+        if (!msg.empty()) return set_error(VK_ERR_INVALID, msg);
+        return VK_OK;
+    });
+}
+
 void vk_pdhg_destroy(vk_pdhg *h) {
     try {
         delete h;

@@ -9,7 +9,7 @@ namespace vk {
 
 struct RunInfo {
     int status = VK_STATUS_NOT_SOLVED;
-    long long iterations = 0, restarts = 0, fp32_iterations = 0;
+    long long iterations = 0, restarts = 0, fp32_iterations = 0, kernel_launches = 0;
     double last_metric = 0.0;
     double iterate_seconds = 0.0;
 };
@@ -22,6 +22,8 @@ public:
     // On return d_xo [n] / d_yo [m] hold the answer in original coordinates.
     virtual void run(const double *d_warm, const double *d_lo, const double *d_hi, double *d_xo, double *d_yo,
                      RunInfo &info, std::chrono::steady_clock::time_point started) = 0;
+    // Per-solve limits and tolerances (the structural options never change).
+    virtual void set_limits(const vk_options &o) = 0;
 };
 
 std::unique_ptr<Engine> make_reference_engine(const DeviceModel &dm, const vk_options &o, cudaStream_t s);

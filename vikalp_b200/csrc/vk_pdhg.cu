@@ -371,6 +371,21 @@ Solver::Solver(const vk_problem &p, const vk_options &o) : opts_(o) {
                                              : make_reference_engine(*dm_, o, stream_);
 }
 
+std::string Solver::set_options(const vk_options &o) {
+    if (o.continuous_method != opts_.continuous_method || o.algorithm != opts_.algorithm ||
+        o.precision != opts_.precision || o.spmv_order != opts_.spmv_order || o.check_every != opts_.check_every ||
+        o.device != opts_.device)
+        return "only limits and tolerances can change after vk_pdhg_create";
+    const bool ok = o.iteration_limit >= 0 && std::isfinite(o.primal_tolerance) && std::isfinite(o.dual_tolerance) &&
+                    o.primal_tolerance >= 0.0 && o.dual_tolerance >= 0.0 && !std::isnan(o.relative_tolerance) &&
+                    o.relative_tolerance >= 0.0 &&
+                    (!std::isfinite(o.time_limit_seconds) || o.time_limit_seconds >= 0.0);
+    if (!ok) return "solver limits and tolerances must be non-negative";
+    opts_ = o;
+    engine_->set_limits(o);
+    return "";
+}
+
 Solver::~Solver() {
     engine_.reset();
     dm_.reset();
@@ -527,6 +542,7 @@ void Solver::solve(const double *warm, const double *lo_ovr, const double *hi_ov
     r->last_metric = info.last_metric;
     r->iterate_seconds = info.iterate_seconds;
     r->fp32_iterations = info.fp32_iterations;
+    r->kernel_launches = info.kernel_launches;
     int status = info.status;
     if (!std::isfinite(obj)) {
         status = VK_STATUS_NUMERICAL_FAILURE;

@@ -325,6 +325,7 @@ public:
                 break;
             }
             VK_CUDA(cudaGraphLaunch(graph_exec_, s_));
+            info.kernel_launches += graph_nodes_;
             VK_CUDA(cudaMemcpyAsync(hctl_.get(), ctl_.get(), sizeof(RefCtl), cudaMemcpyDeviceToHost, s_));
             VK_CUDA(cudaStreamSynchronize(s_));
             check_device_error(s_);
@@ -348,6 +349,8 @@ public:
         if (m > 0) unscale_kernel<<<grid1d(m), 256, 0, s_>>>(y_.get(), rs_.get(), m, d_yo);
         VK_LAUNCH_CHECK();
     }
+
+    void set_limits(const vk_options &o) override { o_ = o; }
 
 private:
     template <class Epi, int NV>
@@ -418,6 +421,9 @@ private:
         for (int k = 0; k < 2 * chunk_; ++k) iteration(k);
         cudaGraph_t g;
         VK_CUDA(cudaStreamEndCapture(s_, &g));
+        size_t nodes = 0;
+        VK_CUDA(cudaGraphGetNodes(g, nullptr, &nodes));
+        graph_nodes_ = static_cast<long long>(nodes);
         VK_CUDA(cudaGraphInstantiate(&graph_exec_, g, 0));
         cudaGraphDestroy(g);
     }
@@ -432,6 +438,7 @@ private:
     HostBuf<RefCtl> hctl_;
     double max_step_ = 0.0;
     int chunk_ = 16;
+    long long graph_nodes_ = 0;
     cudaGraphExec_t graph_exec_ = nullptr;
 };
 

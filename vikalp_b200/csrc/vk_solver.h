@@ -49,6 +49,8 @@ public:
     Solver(const vk_problem &p, const vk_options &o);
     ~Solver();
     void solve(const double *warm, const double *lo, const double *hi, vk_result *r);
+    // Returns "" on success, else the reason the options were not accepted.
+    std::string set_options(const vk_options &o);
     const DeviceModel &model() const { return *dm_; }
     cudaStream_t stream() const { return stream_; }
 
