@@ -170,12 +170,12 @@ def spmv_figures(inst, torch, stream):
     return out
 
 
-def time_to_tolerance(inst, label, limit):
+def time_to_tolerance(inst, label, limit, time_limit=float("inf")):
     import vikalp_b200 as vk
     res = {}
     for prec in ("fp64", "mixed"):
         with vk.Pdhg(inst, algorithm="halpern", precision=prec, iteration_limit=limit,
-                     relative_tolerance=1e-6) as h:
+                     relative_tolerance=1e-6, time_limit_seconds=time_limit) as h:
             r = h.solve(duals=False)
         res[prec] = {"status": r["status"], "iterations": r["iterations"], "fp32_iterations": r["fp32_iterations"],
                      "iterate_s": round(r["iterate_seconds"], 4), "solve_s": round(r["solve_seconds"], 4),
@@ -207,8 +207,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--ttt", action="store_true", help="also time the large LP to 1e-6 relative KKT")
+    ap.add_argument("--ttt-seconds", type=float, default=60.0, help="time cap per precision for --ttt")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--profile-spmv", choices=["fp64", "fp32"], default=None,
+                    help="only run the sparse-product kernel 5 times on the large LP (for ncu captures)")
+    ap.add_argument("--transpose", action="store_true", help="with --profile-spmv: A'y instead of A x")
     args = ap.parse_args()
+    if args.profile_spmv:
+        return profile_spmv(args.profile_spmv, args.transpose)
     K, W = max(1, args.steps), max(3, args.warmup)
     ws, rank, local, dist = dist_setup(args.gpus)
     from vikalp_b200 import synthetic
@@ -298,7 +304,7 @@ def main():
         small = synthetic.workload_small_lp()
         ttt = {"small_lp": time_to_tolerance(small, "lp m=2000 n=5000 nnz=40000", 400000)}
         if args.ttt:
-            ttt["large_lp"] = time_to_tolerance(inst, "large lp", 2_000_000)
+            ttt["large_lp"] = time_to_tolerance(inst, "large lp", 2_000_000, time_limit=args.ttt_seconds)
         line["time_to_tol"] = ttt
         if ws == 1:
             rate, n_it, secs = reference_cpu_rate(inst, budget_s=20.0)
@@ -310,6 +316,25 @@ def main():
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+    return 0
+
+
+def profile_spmv(prec, transpose):
+    """Five launches of the sparse-product kernel (PlainEpi) on the large LP."""
+    import torch
+
+    import vikalp_b200 as vk
+    from vikalp_b200 import synthetic
+    inst = synthetic.workload_large_lp()
+    dt = torch.float64 if prec == "fp64" else torch.float32
+    A = vk.SpMat(inst.row_offsets, inst.col_idx, inst.values, inst.m, inst.n, "fp64" if prec == "fp64" else "mixed")
+    xl, yl = (inst.m, inst.n) if transpose else (inst.n, inst.m)
+    x = torch.rand(xl, dtype=dt, device="cuda")
+    y = torch.zeros(yl, dtype=dt, device="cuda")
+    for _ in range(5):
+        A.apply(x.data_ptr(), y.data_ptr(), transpose, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    print(f"ok variant={A.variant(transpose)} bytes={A.bytes(transpose)}")
     return 0
 
 

@@ -87,7 +87,7 @@ def rel_kkt(inst, x, y, lower=None, upper=None):
 
 
 def solve(inst, tol=1e-6, iteration_limit=100000, check_every=64, rho=1.0, warm=None, lower=None, upper=None,
-          trace=False):
+          trace=False, theta=0.5, omega0=None):
     A = _csr(inst)
     m, n = A.shape
     lo0 = inst.var_lower if lower is None else lower
@@ -106,6 +106,8 @@ def solve(inst, tol=1e-6, iteration_limit=100000, check_every=64, rho=1.0, warm=
     bnorm, cnorm = np.linalg.norm(b_orig), np.linalg.norm(inst.c)
     cs2, bs2 = np.sum(c * c), np.sum((b_orig * r) ** 2)
     omega = np.sqrt(cs2) / np.sqrt(bs2) if (cs2 > 1e-20 and bs2 > 1e-20) else 1.0
+    if omega0 is not None:
+        omega = omega0
     smax = sigma_max(K) if K.nnz else 0.0
     eta = 0.99 / smax if smax > 0 else 1.0
     tau, sigma = eta / omega, eta * omega
@@ -150,7 +152,7 @@ def solve(inst, tol=1e-6, iteration_limit=100000, check_every=64, rho=1.0, warm=
         if restart:
             mx, my = np.sqrt(dx0), np.sqrt(dy0)
             if mx > 1e-10 and my > 1e-10:
-                omega = np.exp(0.5 * np.log(my / mx) + 0.5 * np.log(omega))
+                omega = np.exp(theta * np.log(my / mx) + (1 - theta) * np.log(omega))
             tau, sigma = eta / omega, eta * omega
             k_base = 0
             restarts += 1

@@ -315,8 +315,11 @@ __device__ double block_reduce_range(const double *p, int count, int R, int r, d
     return a[0]; // valid in thread 0
 }
 
-__global__ void check_control_kernel(HalCtl *ctl, const double *pc, const double *pr, const double *pkr,
-                                     const double *pkc, CheckGrids g, int chunk) {
+constexpr int kControlThreads = 256;
+
+__global__ void __launch_bounds__(kControlThreads)
+    check_control_kernel(HalCtl *ctl, const double *pc, const double *pr, const double *pkr, const double *pkc,
+                         CheckGrids g, int chunk) {
     __shared__ double scratch[32];
     __shared__ int skip;
     if (threadIdx.x == 0) skip = ctl->done;
@@ -722,8 +725,8 @@ private:
                 grids.col = col_pass<T, true>(st, it);
                 grids.row = row_pass<T, true>(st, it);
                 grids.kkt_row = kkt_passes(st, grids.kkt_col);
-                check_control_kernel<<<1, 1024, 0, s_>>>(ctl_.get(), pc_.get(), pr_.get(), pkr_.get(), pkc_.get(),
-                                                         grids, chunk_);
+                check_control_kernel<<<1, kControlThreads, 0, s_>>>(ctl_.get(), pc_.get(), pr_.get(), pkr_.get(),
+                                                                    pkc_.get(), grids, chunk_);
                 VK_LAUNCH_CHECK();
                 const int mx = std::max(st.m, st.n);
                 restart_apply_kernel<T><<<grid1d(mx), 256, 0, s_>>>(ctl_.get(), st.x.get(), st.x0.get(),
