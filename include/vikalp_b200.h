@@ -195,6 +195,17 @@ int vk_spmat_variant(const vk_spmat *m, int transpose);
 int vk_spmat_set_variant(vk_spmat *m, int transpose, int variant);
 void vk_spmat_destroy(vk_spmat *m);
 
+/* ExecutionBackend::dot and ::norm_inf on device arrays of n doubles
+ * (ExecutionBackend.hpp:49-51; cuda_ops.cu:407-451), written to
+ * *result_device on `stream` (a cudaStream_t, NULL = default stream). Block
+ * partials go to a per-device scratch buffer this library allocates on first
+ * use (cudaMalloc) and grows as needed; the final sum / max runs on the device
+ * in a fixed order, so results are deterministic. norm_inf ignores NaN
+ * entries, as std::max does in the reference (cpu_ops.cpp:358-364). */
+int vk_vec_dot_device(const double *x_device, const double *y_device, int64_t n, double *result_device,
+                      void *stream);
+int vk_vec_norm_inf_device(const double *x_device, int64_t n, double *result_device, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

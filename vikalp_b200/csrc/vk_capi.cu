@@ -1,6 +1,7 @@
 // extern "C" entry points of include/vikalp_b200.h. Every call catches and
 // maps exceptions to status codes; the message is kept per thread.
 #include "vk_engine.cuh"
+#include "vk_vec.cuh"
 
 #include <cstring>
 #include <memory>
@@ -93,6 +94,11 @@ struct Stream {
 };
 
 } // namespace
+
+namespace vk {
+// Records `msg` as the calling thread's last error and returns `code`.
+int record_error(int code, const std::string &msg) { return set_error(code, msg); }
+} // namespace vk
 
 struct vk_pdhg {
     std::unique_ptr<vk::Solver> solver;
@@ -327,6 +333,24 @@ int vk_spmat_set_variant(vk_spmat *m, int transpose, int variant) {
         return set_error(VK_ERR_INVALID, "variant out of range");
     (transpose ? m->at : m->a).variant = variant;
     return VK_OK;
+}
+
+int vk_vec_dot_device(const double *x, const double *y, int64_t n, double *result, void *stream) {
+    return guarded([&] {
+        if (!result || n < 0 || (n > 0 && (!x || !y))) return set_error(VK_ERR_INVALID, "invalid argument");
+        double *partials = vk::reduction_scratch(std::max<int64_t>(1, vk::reduction_blocks(n)));
+        vk::launch_dot(x, y, n, partials, result, static_cast<cudaStream_t>(stream));
+        return VK_OK;
+    });
+}
+
+int vk_vec_norm_inf_device(const double *x, int64_t n, double *result, void *stream) {
+    return guarded([&] {
+        if (!result || n < 0 || (n > 0 && !x)) return set_error(VK_ERR_INVALID, "invalid argument");
+        double *partials = vk::reduction_scratch(std::max<int64_t>(1, vk::reduction_blocks(n)));
+        vk::launch_norm_inf(x, n, partials, result, static_cast<cudaStream_t>(stream));
+        return VK_OK;
+    });
 }
 
 void vk_spmat_destroy(vk_spmat *m) {
