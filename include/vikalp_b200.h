@@ -206,6 +206,21 @@ int vk_vec_dot_device(const double *x_device, const double *y_device, int64_t n,
                       void *stream);
 int vk_vec_norm_inf_device(const double *x_device, int64_t n, double *result_device, void *stream);
 
+/* vk_vec_dot_device for callers that cannot allocate device memory (a
+ * framework allocator or memory pool owns every byte, or the process has a
+ * fixed memory budget): the same kernels and the same result, with the block
+ * partials in a 32 KB array compiled into the library instead of a buffer
+ * allocated by cudaMalloc. No counterpart in the reference. It never calls
+ * cudaMalloc or cudaFree. Limits and caveats:
+ *   - n <= 8388608 (4096 block partials); larger n returns VK_ERR_INVALID;
+ *   - every GPU that loads the library holds the array until the process
+ *     exits, and all calls share it: calls that overlap on the GPU (other
+ *     streams or host threads) race and may return wrong sums;
+ *   - the first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress); make that call before any stream capture. */
+int vk_vec_dot_device_noalloc(const double *x_device, const double *y_device, int64_t n, double *result_device,
+                              void *stream);
+
 #ifdef __cplusplus
 }
 #endif

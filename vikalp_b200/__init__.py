@@ -92,6 +92,7 @@ _SIGNATURES = {
     "vk_spmat_destroy": (None, [C.c_void_p]),
     "vk_vec_dot_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "vk_vec_norm_inf_device": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
+    "vk_vec_dot_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None
