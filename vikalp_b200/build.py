@@ -67,9 +67,29 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False, e
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    build_host(force=force)
     if verbose:
-        print(f"built {LIB} ({len(todo)} objects recompiled)")
+        print(f"built {LIB} ({len(todo)} objects recompiled) and {HOST_LIB}")
     return LIB
+
+
+HOST_LIB = os.path.join(PKG, "libvikalp.so")
+CXX = os.environ.get("CXX", "g++")
+
+
+def build_host(force: bool = False) -> str:
+    """The C++20 host layer (vikalp::solve and the contracts) over the C ABI."""
+    srcs = sorted(glob.glob(os.path.join(PKG, "host", "*.cpp")))
+    hdrs = glob.glob(os.path.join(ROOT, "include", "**", "*.h*"), recursive=True)
+    newest = max([os.path.getmtime(p) for p in srcs + hdrs + [LIB]], default=0.0)
+    if not force and os.path.exists(HOST_LIB) and os.path.getmtime(HOST_LIB) >= newest:
+        return HOST_LIB
+    cmd = [CXX, "-std=c++20", "-O2", "-fPIC", "-shared", "-I", os.path.join(ROOT, "include"), *srcs,
+           "-L", PKG, "-lvikalp_b200", "-Wl,-rpath,$ORIGIN", "-o", HOST_LIB]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"host build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return HOST_LIB
 
 
 def main(argv=None) -> int:
