@@ -221,6 +221,23 @@ int vk_vec_norm_inf_device(const double *x_device, int64_t n, double *result_dev
 int vk_vec_dot_device_noalloc(const double *x_device, const double *y_device, int64_t n, double *result_device,
                               void *stream);
 
+/* ---- batches ---------------------------------------------------------------- */
+
+/* Solves `count` independent LPs (any sizes) together with VK_ALGO_HALPERN
+ * (opts->algorithm must be VK_ALGO_HALPERN; NULL opts = defaults with that
+ * algorithm). Replaces a loop of vikalp::solve calls, one per model
+ * (Solver.hpp:19-21; the reference has no batch entry point). Every problem is
+ * validated with vk_pdhg_create's rules (an invalid one fails the whole call
+ * with its index in the message); quadratic objectives are VK_ERR_UNSUPPORTED.
+ * The instances share the device passes (one launch advances all of them) but
+ * keep their own step sizes, primal weights, restarts and stopping, so each
+ * result[b] equals, up to rounding, what one VK_ALGO_HALPERN solve of
+ * problem b returns. results[b] receives x, y, status, iterations, restarts,
+ * objective and the relative KKT figures; the duals split and the absolute
+ * residuals are not computed (NaN). iterate_seconds and kernel_launches cover
+ * the whole batch. */
+int vk_batch_solve(const vk_problem *problems, int32_t count, const vk_options *opts, vk_result *results);
+
 #ifdef __cplusplus
 }
 #endif

@@ -79,7 +79,7 @@ def rel_kkt(inst, x, y, lower=None, upper=None):
     vl, vu = np.maximum(0, lam), np.maximum(0, -lam)
     viol = np.sum(np.where((yl > 0) & ~np.isfinite(rl), yl, 0) ** 2) + np.sum(np.where((yu > 0) & ~np.isfinite(ru), yu, 0) ** 2)
     rd2 = np.sum(np.where((vl > 0) & ~np.isfinite(lo), vl, 0) ** 2) + np.sum(np.where((vu > 0) & ~np.isfinite(hi), vu, 0) ** 2)
-    fin = lambda v, w: np.where((w > 0) & np.isfinite(v), v * w, 0.0)  # noqa: E731
+    fin = lambda v, w: np.where((w > 0) & np.isfinite(v), np.where(np.isfinite(v), v, 0.0) * w, 0.0)  # noqa: E731
     dobj = np.sum(fin(rl, yl)) - np.sum(fin(ru, yu)) + np.sum(fin(lo, vl)) - np.sum(fin(hi, vu))
     pobj = inst.c @ x
     return dict(rel_primal=rp / (1 + np.linalg.norm(b)), rel_dual=np.sqrt(rd2 + viol) / (1 + np.linalg.norm(inst.c)),
@@ -135,7 +135,7 @@ def solve(inst, tol=1e-6, iteration_limit=100000, check_every=64, rho=1.0, warm=
         kk = rel_kkt(inst, xh * d, yh * r, lo0, hi0)
         kkt = max(kk["rel_primal"], kk["rel_dual"], kk["rel_gap"])
         if trace:
-            hist.append((total, kkt, restarts, omega))
+            hist.append((total, kkt, restarts, omega, kk["rel_primal"], kk["rel_dual"], kk["rel_gap"]))
         if kkt <= tol:
             status = "Optimal"
             break

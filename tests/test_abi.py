@@ -147,3 +147,24 @@ def test_large_psd_gate_rejects_indefinite():
           q_values=d)
     code, msg = create_error(m)
     assert code == vk.VK_ERR_UNSUPPORTED and msg == "QP objective matrix is not positive semidefinite"
+
+
+def batch_error(models, **opts):
+    with pytest.raises(vk.VkError) as e:
+        vk.batch_solve(models, **opts)
+    return e.value.code, e.value.msg
+
+
+def test_batch_names_the_invalid_member():
+    code, msg = batch_error([M(), M(var_lower=np.array([3.0]), var_upper=np.array([2.0]))])
+    assert code == vk.VK_ERR_INVALID
+    assert msg == "instance 1: variable bounds contains an invalid bound at index 0"
+
+
+def test_batch_requires_halpern_and_lp():
+    code, _ = batch_error([M()], algorithm="reference")
+    assert code == vk.VK_ERR_UNSUPPORTED
+    q = M(q_row_offsets=np.array([0, 1], np.int64), q_col_idx=np.array([0], np.int64), q_values=np.array([1.0]))
+    code, msg = batch_error([M(), q])
+    assert code == vk.VK_ERR_UNSUPPORTED and msg.startswith("instance 1")
+    assert vk.lib().vk_batch_solve(None, 0, None, None) == vk.VK_ERR_INVALID

@@ -1,0 +1,111 @@
+"""Independent LPs solved as one batch (vk_batch_solve) on the GPU.
+
+* per-instance iterate agreement with the NumPy restatement of the Halpern
+  scheme (oracle/halpern.py) after 128 iterations (two checks, one restart
+  decision each), to 1e-8 relative: each instance of the batch must follow its
+  own single-instance trajectory (own scaling, step size, primal weight);
+* every instance solved to relative KKT <= 1e-6 as evaluated by the C oracle
+  from the returned (x, y) (tolerance written here: 1.05e-6, sums reordered),
+  with the objective within 1e-6 relative of HiGHS -- float64 and mixed;
+* degenerate members (a 1x1 LP, an LP with an empty row and an empty column)
+  and members that converge at very different times (tiles of finished
+  instances are skipped, which must leave their answers untouched).
+"""
+
+import numpy as np
+import pytest
+
+import vikalp_b200 as vk
+from oracle import halpern
+from oracle.highs import objective as highs_objective
+from vikalp_b200 import synthetic
+
+pytestmark = pytest.mark.gpu
+
+KKT_TOL = 1.05e-6
+
+
+@pytest.fixture(scope="module")
+def members():
+    return [synthetic.lp_uniform(200, 500, 6, seed=11), synthetic.lp_uniform(600, 1500, 6, seed=77),
+            synthetic.lp_uniform(40, 90, 4, seed=5), synthetic.lp_uniform(1200, 2400, 8, seed=13),
+            synthetic.lp_uniform(300, 800, 5, seed=3)]
+
+
+def _degenerate():
+    one = synthetic.Instance(m=1, n=1, row_offsets=np.array([0, 1], np.int64), col_idx=np.array([0], np.int64),
+                             values=np.array([2.0]), c=np.array([-1.0]), var_lower=np.array([0.0]),
+                             var_upper=np.array([10.0]), row_lower=np.array([-np.inf]), row_upper=np.array([4.0]),
+                             x0=np.array([1.0]), name="1x1")
+    base = synthetic.lp_uniform(50, 120, 4, seed=21)
+    # drop row 7 (empty row) and every entry of column 3 (empty column)
+    ro, ci, v = base.row_offsets, base.col_idx, base.values
+    keep = np.ones(base.nnz, bool)
+    keep[ro[7]:ro[8]] = False
+    keep &= ci != 3
+    rows = np.repeat(np.arange(base.m), np.diff(ro))[keep]
+    new_ro = np.zeros(base.m + 1, np.int64)
+    np.add.at(new_ro, rows + 1, 1)
+    new_ro = np.cumsum(new_ro)
+    inst = synthetic.Instance(m=base.m, n=base.n, row_offsets=new_ro, col_idx=ci[keep].copy(), values=v[keep].copy(),
+                              c=base.c.copy(), var_lower=base.var_lower.copy(), var_upper=base.var_upper.copy(),
+                              row_lower=base.row_lower.copy(), row_upper=base.row_upper.copy(), x0=base.x0,
+                              name="holes")
+    ax = synthetic.csr_matvec(inst.row_offsets, inst.col_idx, inst.values, base.x0)
+    inst.row_lower = np.where(np.isfinite(inst.row_lower), np.minimum(inst.row_lower, ax), inst.row_lower)
+    inst.row_upper = np.maximum(inst.row_upper, ax)
+    inst.row_lower[7], inst.row_upper[7] = -1.0, 1.0
+    return [one, inst]
+
+
+def test_batch_follows_each_single_trajectory(members):
+    outs = vk.batch_solve(members, iteration_limit=128, relative_tolerance=0.0, check_every=64)
+    for inst, got in zip(members, outs):
+        want = halpern.solve(inst, tol=0.0, iteration_limit=128, check_every=64)
+        assert got["iterations"] == want["iterations"] == 128
+        assert got["restarts"] == want["restarts"]
+        for k in ("x", "y"):
+            scale = 1.0 + np.abs(want[k]).max()
+            assert np.max(np.abs(got[k] - want[k])) <= 1e-8 * scale, (inst.name, k)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_solves_every_member(members, oracle, precision):
+    outs = vk.batch_solve(members, precision=precision, iteration_limit=200000, relative_tolerance=1e-6)
+    iters = []
+    for inst, r in zip(members, outs):
+        assert r["status"] == "Optimal", inst.name
+        k = oracle.rel_kkt(inst, r["x"], r["y"])
+        assert max(k["rel_primal"], k["rel_dual"], k["rel_gap"]) <= KKT_TOL, (inst.name, k)
+        assert max(r["rel_primal"], r["rel_dual"], r["rel_gap"]) <= KKT_TOL
+        ref = highs_objective(inst)
+        assert abs(r["objective"] - ref) <= 1e-6 * (1 + abs(ref)), inst.name
+        iters.append(r["iterations"])
+    # members stop on their own schedules
+    assert len(set(iters)) > 1
+
+
+def test_batch_matches_single_solves(members):
+    outs = vk.batch_solve(members, iteration_limit=200000, relative_tolerance=1e-6)
+    for inst, r in zip(members, outs):
+        s = vk.solve(inst, algorithm="halpern", iteration_limit=200000, relative_tolerance=1e-6)
+        assert s["status"] == r["status"] == "Optimal"
+        # same scheme, sums reordered: the stopping check may land one chunk apart
+        assert abs(s["iterations"] - r["iterations"]) <= 64 * 4, inst.name
+        assert abs(s["objective"] - r["objective"]) <= 2e-6 * (1 + abs(s["objective"]))
+
+
+def test_batch_degenerate_members(oracle):
+    insts = _degenerate() + [synthetic.lp_uniform(100, 250, 5, seed=9)]
+    outs = vk.batch_solve(insts, iteration_limit=200000, relative_tolerance=1e-6)
+    for inst, r in zip(insts, outs):
+        assert r["status"] == "Optimal", inst.name
+        k = oracle.rel_kkt(inst, r["x"], r["y"])
+        assert max(k["rel_primal"], k["rel_dual"], k["rel_gap"]) <= KKT_TOL, (inst.name, k)
+        assert abs(r["objective"] - highs_objective(inst)) <= 1e-6 * (1 + abs(r["objective"])), inst.name
+    assert abs(outs[0]["x"][0] - 2.0) <= 1e-5
+
+
+def test_batch_limits(members):
+    outs = vk.batch_solve(members, iteration_limit=64, relative_tolerance=1e-12)
+    assert all(r["status"] == "IterationLimit" and r["iterations"] == 64 for r in outs)

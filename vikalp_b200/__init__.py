@@ -93,6 +93,7 @@ _SIGNATURES = {
     "vk_vec_dot_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "vk_vec_norm_inf_device": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "vk_vec_dot_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
+    "vk_batch_solve": (C.c_int, [C.POINTER(Problem), C.c_int32, C.POINTER(Options), C.POINTER(Result)]),
 }
 
 _lib = None
@@ -241,6 +242,27 @@ def solve(inst, warm=None, lower=None, upper=None, **opts) -> dict:
     """Create + solve + destroy: the one-shot C-ABI route."""
     with Pdhg(inst, **opts) as h:
         return h.solve(warm, lower, upper)
+
+
+def batch_solve(instances, **opts) -> list[dict]:
+    """Independent LPs in one batch (vk_batch_solve); one result dict per instance."""
+    opts.setdefault("algorithm", "halpern")
+    keep = _Keep()
+    probs = (Problem * len(instances))(*[problem_struct(inst, keep) for inst in instances])
+    results = (Result * len(instances))()
+    outs = []
+    for inst, r in zip(instances, results):
+        o = {"x": np.zeros(inst.n), "y": np.zeros(inst.m)}
+        r.x, r.y = _p(o["x"]), _p(o["y"])
+        outs.append(o)
+    o = options(**opts)
+    _check(lib().vk_batch_solve(probs, len(instances), C.byref(o), results))
+    for out, r in zip(outs, results):
+        out.update(status=STATUS.get(r.status, str(r.status)), iterations=r.iterations, restarts=r.restarts,
+                   objective=r.objective, rel_primal=r.rel_primal, rel_dual=r.rel_dual, rel_gap=r.rel_gap,
+                   last_metric=r.last_metric, solve_seconds=r.solve_seconds, iterate_seconds=r.iterate_seconds,
+                   fp32_iterations=r.fp32_iterations, kernel_launches=r.kernel_launches)
+    return outs
 
 
 def spmv(ro, ci, v, rows, cols, x, y=None, alpha=1.0, beta=0.0, transpose=False, order="fast"):

@@ -1,0 +1,1030 @@
+// Batched restarted-Halpern PDHG over many independent LPs of uneven size.
+//
+// The instances are laid out as one block-diagonal problem (rows, columns and
+// nonzeros concatenated; warp-tiles never cross an instance), so one launch of
+// each fused pass advances every instance. Each instance keeps its own step
+// size eta_b (power iteration run on all instances at once, normalised per
+// instance), primal weight omega_b, Halpern counter, restart state and
+// convergence mask: per-row / per-column epilogues look their instance up, and
+// the tiles of an instance that has converged are skipped, so a draining
+// batch stops streaming the finished instances. Check reductions are written
+// per tile and summed per instance in a fixed order (deterministic); a
+// control kernel with one thread per instance applies the same stop / restart
+// / primal-weight rules as the single-instance engine (vk_halpern.cu). The
+// chunk of check_every iterations is one CUDA graph.
+#include "vk_engine.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <numeric>
+
+namespace vk {
+namespace {
+
+constexpr double kRhoB = 1.0;
+constexpr int kRuizB = 10;
+
+// Per-instance control, structure of arrays (device).
+struct BCtl {
+    double *eta, *omega, *tau, *sigma, *r_restart, *r_prev, *bnorm, *cnorm, *offset, *kkt, *rel_p, *rel_d, *rel_gap;
+    long long *k_base, *iters, *restarts;
+    int *done, *status, *restart_now;
+    double tol;
+    long long limit;
+    int count;
+};
+
+__device__ __forceinline__ double lam_of(const BCtl &c, int b, int it) {
+    const double k = static_cast<double>(c.k_base[b] + it);
+    return (k + 1.0) / (k + 2.0);
+}
+
+template <class T, bool CHECK>
+struct BColEpi : EpiBase<T> {
+    static constexpr int NR = CHECK ? 2 : 1;
+    static constexpr bool kPerTile = CHECK;
+    BCtl ctl;
+    int it;
+    const int *inst, *tile_inst;
+    T *x, *xbar, *xhat;
+    const T *x0, *c, *l, *u;
+    double *partials;
+    struct Pre {
+        T x, x0, c, l, u;
+        int b;
+    };
+    __device__ bool skip_tile(int t) const { return ctl.done[tile_inst[t]] != 0; }
+    __device__ Pre load(int j) const { return Pre{x[j], x0[j], c[j], l[j], u[j], inst[j]}; }
+    __device__ void row_pre(int j, const T (&s)[1], const Pre &p, double (&red)[NR]) const {
+        const T tau = static_cast<T>(ctl.tau[p.b]);
+        const T lam = static_cast<T>(lam_of(ctl, p.b, it));
+        const T xh = clampbox(p.x - tau * (p.c + s[0]), p.l, p.u);
+        xbar[j] = T(2) * xh - p.x;
+        x[j] = lam * ((T(1) + T(kRhoB)) * xh - T(kRhoB) * p.x) + (T(1) - lam) * p.x0;
+        if (CHECK) {
+            xhat[j] = xh;
+            const double d0 = static_cast<double>(xh) - static_cast<double>(p.x);
+            const double d1 = static_cast<double>(xh) - static_cast<double>(p.x0);
+            red[0] += d0 * d0;
+            red[CHECK ? 1 : 0] += d1 * d1;
+        }
+    }
+    template <int R>
+    __device__ void tile_done(int t, double (&red)[R]) const {
+        for (int r = 0; r < R; ++r) partials[(size_t)t * R + r] = red[r];
+    }
+};
+
+template <class T, bool CHECK>
+struct BRowEpi : EpiBase<T> {
+    static constexpr int NR = CHECK ? 2 : 1;
+    static constexpr bool kPerTile = CHECK;
+    BCtl ctl;
+    int it;
+    const int *inst, *tile_inst;
+    T *y, *yhat;
+    const T *y0, *rl, *ru;
+    double *partials;
+    struct Pre {
+        T y, y0, rl, ru;
+        int b;
+    };
+    __device__ bool skip_tile(int t) const { return ctl.done[tile_inst[t]] != 0; }
+    __device__ Pre load(int i) const { return Pre{y[i], y0[i], rl[i], ru[i], inst[i]}; }
+    __device__ void row_pre(int i, const T (&s)[1], const Pre &p, double (&red)[NR]) const {
+        const T sigma = static_cast<T>(ctl.sigma[p.b]);
+        const T lam = static_cast<T>(lam_of(ctl, p.b, it));
+        const T v = p.y + sigma * s[0];
+        const T yh = v - clampbox(v, sigma * p.rl, sigma * p.ru);
+        y[i] = lam * ((T(1) + T(kRhoB)) * yh - T(kRhoB) * p.y) + (T(1) - lam) * p.y0;
+        if (CHECK) {
+            yhat[i] = yh;
+            const double d0 = static_cast<double>(yh) - static_cast<double>(p.y);
+            const double d1 = static_cast<double>(yh) - static_cast<double>(p.y0);
+            red[0] += d0 * d0;
+            red[CHECK ? 1 : 0] += d1 * d1;
+        }
+    }
+    template <int R>
+    __device__ void tile_done(int t, double (&red)[R]) const {
+        for (int r = 0; r < R; ++r) partials[(size_t)t * R + r] = red[r];
+    }
+};
+
+template <class T>
+struct BKktRowEpi : EpiBase<T> {
+    static constexpr int NR = 3;
+    static constexpr bool kPerTile = true;
+    BCtl ctl;
+    const int *tile_inst;
+    const T *yhat, *rl, *ru, *rs;
+    double *partials;
+    struct Pre {
+        T y, rl, ru, r;
+    };
+    __device__ bool skip_tile(int t) const { return ctl.done[tile_inst[t]] != 0; }
+    __device__ Pre load(int i) const { return Pre{yhat[i], rl[i], ru[i], rs[i]}; }
+    __device__ void row_pre(int, const T (&s)[1], const Pre &p, double (&red)[NR]) const {
+        const double a = static_cast<double>(s[0]);
+        const double lo = static_cast<double>(p.rl), hi = static_cast<double>(p.ru), r = static_cast<double>(p.r);
+        const double pr = (a - clampbox(a, lo, hi)) / r;
+        red[0] += pr * pr;
+        const double y = static_cast<double>(p.y);
+        const double yl = smax(0.0, -y), yu = smax(0.0, y);
+        if (yl > 0.0) {
+            if (isfinite(lo)) red[1] += lo * yl; else red[2] += (r * yl) * (r * yl);
+        }
+        if (yu > 0.0) {
+            if (isfinite(hi)) red[1] -= hi * yu; else red[2] += (r * yu) * (r * yu);
+        }
+    }
+    template <int R>
+    __device__ void tile_done(int t, double (&red)[R]) const {
+        for (int r = 0; r < R; ++r) partials[(size_t)t * R + r] = red[r];
+    }
+};
+
+template <class T>
+struct BKktColEpi : EpiBase<T> {
+    static constexpr int NR = 4;
+    static constexpr bool kPerTile = true;
+    BCtl ctl;
+    const int *tile_inst;
+    const T *xhat, *c, *l, *u, *cs;
+    double *partials;
+    struct Pre {
+        T x, c, l, u, d;
+    };
+    __device__ bool skip_tile(int t) const { return ctl.done[tile_inst[t]] != 0; }
+    __device__ Pre load(int j) const { return Pre{xhat[j], c[j], l[j], u[j], cs[j]}; }
+    __device__ void row_pre(int, const T (&s)[1], const Pre &p, double (&red)[NR]) const {
+        const double lam = static_cast<double>(p.c) + static_cast<double>(s[0]);
+        const double d = static_cast<double>(p.d);
+        const double lo = static_cast<double>(p.l), hi = static_cast<double>(p.u), x = static_cast<double>(p.x);
+        const double vl = smax(0.0, lam), vu = smax(0.0, -lam);
+        if (vl > 0.0) {
+            if (isfinite(lo)) red[1] += lo * vl; else red[0] += (vl / d) * (vl / d);
+        }
+        if (vu > 0.0) {
+            if (isfinite(hi)) red[1] -= hi * vu; else red[0] += (vu / d) * (vu / d);
+        }
+        red[2] += static_cast<double>(p.c) * x;
+        const double bx = (x - clampbox(x, lo, hi)) * d;
+        red[3] += bx * bx;
+    }
+    template <int R>
+    __device__ void tile_done(int t, double (&red)[R]) const {
+        for (int r = 0; r < R; ++r) partials[(size_t)t * R + r] = red[r];
+    }
+};
+
+template <class T>
+struct BStore : EpiRow<T, BStore<T>> {
+    T *y;
+    __device__ void row(int i, const T (&s)[1], double (&)[1]) const { y[i] = s[0]; }
+};
+
+// out[b*R + r] = sum of partials over tiles [begin[b], begin[b+1]) (fixed order).
+__global__ void segment_reduce_kernel(const double *__restrict__ partials, const int *__restrict__ begin, int count,
+                                      int R, double *__restrict__ out) {
+    const int b = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (b >= count) return;
+    for (int r = 0; r < R; ++r) {
+        double s = 0.0;
+        for (int t = begin[b] + lane; t < begin[b + 1]; t += 32) s += partials[(size_t)t * R + r];
+        s = warp_sum(s);
+        if (lane == 0) out[(size_t)b * R + r] = s;
+    }
+}
+
+// out[b] = sum_{i in segment b} a_i * a_i (contiguous segments; one warp each).
+template <class T>
+__global__ void segment_norm2_kernel(const T *__restrict__ a, const int *__restrict__ off, int count,
+                                     double *__restrict__ out) {
+    const int b = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (b >= count) return;
+    double s = 0.0;
+    for (int i = off[b] + lane; i < off[b + 1]; i += 32) s += static_cast<double>(a[i]) * static_cast<double>(a[i]);
+    s = warp_sum(s);
+    if (lane == 0) out[b] = s;
+}
+
+template <class T>
+__global__ void segment_scale_kernel(T *__restrict__ a, const int *__restrict__ inst, int n,
+                                     const double *__restrict__ nrm2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = nrm2[inst[i]];
+    if (v > 0.0) a[i] = static_cast<T>(a[i] / sqrt(v));
+}
+
+__global__ void bscaled_norm_kernel(const int *__restrict__ ro, const int *__restrict__ ci,
+                                    const double *__restrict__ v, const double *__restrict__ self,
+                                    const double *__restrict__ other, int rows, int mode, double *__restrict__ out) {
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= rows) return;
+    double acc = 0.0;
+    for (int k = ro[r] + lane; k < ro[r + 1]; k += 32) {
+        const double a = fabs(v[k]) * other[ci[k]];
+        acc = mode == 0 ? fmax(acc, a) : acc + a;
+    }
+    acc = mode == 0 ? warp_max_nonneg(acc) : warp_sum(acc);
+    if (lane == 0) out[r] = acc * self[r];
+}
+
+__global__ void brescale_kernel(double *__restrict__ s, const double *__restrict__ norm, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && norm[i] > 0.0) s[i] /= sqrt(norm[i]);
+}
+
+template <class T>
+__global__ void bscale_matrix_kernel(const int *__restrict__ ro, const int *__restrict__ ci,
+                                     const double *__restrict__ v, const double *__restrict__ rs,
+                                     const double *__restrict__ cs, int rows, bool transposed, T *__restrict__ out) {
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= rows) return;
+    for (int k = ro[r] + lane; k < ro[r + 1]; k += 32) {
+        const int c = ci[k];
+        out[k] = static_cast<T>(transposed ? v[k] * rs[c] * cs[r] : v[k] * rs[r] * cs[c]);
+    }
+}
+
+template <class T>
+__global__ void bscale_vec_kernel(const double *__restrict__ a, const double *__restrict__ s, int n, int mode,
+                                  T *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = a[i];
+    double r;
+    if (mode == 0)
+        r = v * s[i];
+    else if (!isfinite(v))
+        r = v;
+    else
+        r = mode == 1 ? v / s[i] : v * s[i];
+    out[i] = static_cast<T>(r);
+}
+
+template <class TD, class TS>
+__global__ void bconvert_kernel(const TS *__restrict__ a, int n, TD *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = static_cast<TD>(a[i]);
+}
+
+// Power-iteration start vector: the single-instance engine's hash of the
+// column index, taken per instance (local index), so both start alike.
+__global__ void bseed_kernel(double *a, const int *__restrict__ inst, const int *__restrict__ off, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        unsigned h = static_cast<unsigned>(i - off[inst[i]]) * 2654435761u + 12345u;
+        h ^= h >> 13;
+        h *= 2246822519u;
+        h ^= h >> 16;
+        a[i] = 0.5 + static_cast<double>(h & 0xffff) / 65536.0;
+    }
+}
+
+// One thread per instance: the single-instance check rules (vk_halpern.cu).
+__global__ void batch_control_kernel(BCtl c, const double *cs, const double *rs, const double *kr, const double *kc,
+                                     int chunk) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= c.count || c.done[b]) return;
+    const double dx2 = cs[b * 2], dx0 = cs[b * 2 + 1], dy2 = rs[b * 2], dy0 = rs[b * 2 + 1];
+    const double rp2 = kr[b * 3], dobj_r = kr[b * 3 + 1], viol2 = kr[b * 3 + 2];
+    const double rd2 = kc[b * 4], dobj_c = kc[b * 4 + 1], pobj = kc[b * 4 + 2] + c.offset[b], box2 = kc[b * 4 + 3];
+    const double dobj = dobj_r + dobj_c + c.offset[b];
+    c.iters[b] += chunk;
+    c.rel_p[b] = (sqrt(rp2) + sqrt(box2)) / (1.0 + c.bnorm[b]);
+    c.rel_d[b] = sqrt(rd2 + viol2) / (1.0 + c.cnorm[b]);
+    c.rel_gap[b] = fabs(pobj - dobj) / (1.0 + fabs(pobj) + fabs(dobj));
+    const double kkt = smax(smax(c.rel_p[b], c.rel_d[b]), c.rel_gap[b]);
+    c.kkt[b] = kkt;
+    c.restart_now[b] = 0;
+    if (!(kkt == kkt)) {
+        c.done[b] = 1;
+        c.status[b] = VK_STATUS_NUMERICAL_FAILURE;
+        return;
+    }
+    if (kkt <= c.tol) {
+        c.done[b] = 1;
+        c.status[b] = VK_STATUS_OPTIMAL;
+        return;
+    }
+    if (c.iters[b] >= c.limit) {
+        c.done[b] = 1;
+        c.status[b] = VK_STATUS_ITERATION_LIMIT;
+        return;
+    }
+    const double omega = c.omega[b];
+    const double r = sqrt(omega * dx2 + dy2 / omega);
+    const long long k = c.k_base[b] + chunk;
+    bool restart = false;
+    if (c.r_restart[b] < 0.0) {
+        c.r_restart[b] = r;
+    } else {
+        restart = (r <= 0.2 * c.r_restart[b]) || (r <= 0.8 * c.r_restart[b] && r > c.r_prev[b]) ||
+                  (static_cast<double>(k) >= 0.36 * static_cast<double>(c.iters[b]));
+    }
+    c.r_prev[b] = r;
+    if (restart) {
+        const double mx = sqrt(dx0), my = sqrt(dy0);
+        double w = omega;
+        if (mx > 1e-10 && my > 1e-10) w = exp(0.5 * log(my / mx) + 0.5 * log(omega));
+        c.omega[b] = w;
+        c.tau[b] = c.eta[b] / w;
+        c.sigma[b] = c.eta[b] * w;
+        c.k_base[b] = 0;
+        c.restarts[b] += 1;
+        c.restart_now[b] = 1;
+        c.r_restart[b] = r;
+    } else {
+        c.k_base[b] = k;
+    }
+}
+
+template <class T>
+__global__ void brestart_kernel(BCtl c, const int *ci, const int *ri, T *x, T *x0, const T *xhat, int n, T *y, T *y0,
+                                const T *yhat, int m) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int b = ci[i];
+        if (c.restart_now[b] && !c.done[b]) {
+            x[i] = xhat[i];
+            x0[i] = xhat[i];
+        }
+    }
+    if (i < m) {
+        const int b = ri[i];
+        if (c.restart_now[b] && !c.done[b]) {
+            y[i] = yhat[i];
+            y0[i] = yhat[i];
+        }
+    }
+}
+
+template <class T>
+__global__ void bunscale_kernel(const T *__restrict__ a, const double *__restrict__ s, int n, double *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = static_cast<double>(a[i]) * s[i];
+}
+
+template <class T>
+struct BState {
+    DevBuf<T> ka, kat, c, l, u, rl, ru, rs, cs, x, x0, xbar, xhat, y, y0, yhat;
+};
+
+class BatchEngine {
+public:
+    BatchEngine(const vk_problem *probs, int count, const vk_options &o) : o_(o), B_(count) {
+        VK_CUDA(cudaSetDevice(o.device));
+        device_error_flag();
+        VK_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
+        mixed_ = o.precision == VK_PREC_MIXED;
+        chunk_ = std::max(2, o.check_every > 0 ? o.check_every : 64);
+        concatenate(probs);
+        setup_device();
+    }
+    ~BatchEngine() {
+        if (g64_) cudaGraphExecDestroy(g64_);
+        if (g32_) cudaGraphExecDestroy(g32_);
+        if (s_) cudaStreamDestroy(s_);
+    }
+
+    void solve(vk_result *results) {
+        const auto started = std::chrono::steady_clock::now();
+        reset_control();
+        cudaEvent_t e0, e1;
+        VK_CUDA(cudaEventCreate(&e0));
+        VK_CUDA(cudaEventCreate(&e1));
+        VK_CUDA(cudaEventRecord(e0, s_));
+        long long launches = 0, fp32_iters = 0;
+        bool timed_out = false;
+        if (mixed_) {
+            copy_state<float, double>(s64_, s32_, true);
+            if (!g32_) g32_ = capture(s32_);
+            std::vector<double> best(B_, std::numeric_limits<double>::infinity());
+            int stall = 0;
+            for (;;) {
+                if (over_time(started)) {
+                    timed_out = true;
+                    break;
+                }
+                VK_CUDA(cudaGraphLaunch(g32_, s_));
+                launches += nodes_;
+                read_control();
+                check_device_error(s_);
+                bool improved = false, all_done = true;
+                double worst = 0.0;
+                for (int b = 0; b < B_; ++b) {
+                    if (h_done_[b]) continue;
+                    all_done = false;
+                    worst = std::max(worst, h_kkt_[b]);
+                    if (h_kkt_[b] < 0.7 * best[b]) {
+                        best[b] = h_kkt_[b];
+                        improved = true;
+                    }
+                }
+                if (all_done) break;
+                if (improved)
+                    stall = 0;
+                else if (++stall >= 6 && worst < 1e-3)
+                    break;
+            }
+            fp32_iters = *std::max_element(h_iters_.begin(), h_iters_.end());
+            copy_state<double, float>(s32_, s64_, false);
+            // re-open every instance that stopped on the float32 measurement
+            reopen_after_fp32();
+        }
+        if (!timed_out) {
+            if (!g64_) g64_ = capture(s64_);
+            for (;;) {
+                if (over_time(started)) {
+                    timed_out = true;
+                    break;
+                }
+                VK_CUDA(cudaGraphLaunch(g64_, s_));
+                launches += nodes_;
+                read_control();
+                check_device_error(s_);
+                if (std::all_of(h_done_.begin(), h_done_.end(), [](int d) { return d != 0; })) break;
+            }
+        }
+        VK_CUDA(cudaEventRecord(e1, s_));
+        read_control();
+        float ms = 0.f;
+        VK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        // answers: (x^, y^) of the last check, unscaled
+        DevBuf<double> xo(n_), yo(m_ > 0 ? m_ : 1);
+        bunscale_kernel<double><<<grid1d(n_), 256, 0, s_>>>(s64_.xhat.get(), cs_.get(), n_, xo.get());
+        if (m_ > 0) bunscale_kernel<double><<<grid1d(m_), 256, 0, s_>>>(s64_.yhat.get(), rs_.get(), m_, yo.get());
+        VK_LAUNCH_CHECK();
+        std::vector<double> hx(n_), hy(m_);
+        VK_CUDA(cudaMemcpyAsync(hx.data(), xo.get(), n_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
+        if (m_ > 0) VK_CUDA(cudaMemcpyAsync(hy.data(), yo.get(), m_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaStreamSynchronize(s_));
+        const double secs = seconds_since(started);
+        for (int b = 0; b < B_; ++b) {
+            vk_result &r = results[b];
+            const int c0 = col_off_[b], c1 = col_off_[b + 1], r0 = row_off_[b], r1 = row_off_[b + 1];
+            if (r.x) std::copy(hx.begin() + c0, hx.begin() + c1, r.x);
+            if (r.y) std::copy(hy.begin() + r0, hy.begin() + r1, r.y);
+            double obj = offset_[b];
+            for (int j = c0; j < c1; ++j) obj += h_c_[j] * hx[j];
+            r.objective = obj;
+            r.status = h_done_[b] ? h_status_[b] : (timed_out ? VK_STATUS_TIME_LIMIT : VK_STATUS_ITERATION_LIMIT);
+            r.iterations = h_iters_[b];
+            r.restarts = h_restarts_[b];
+            r.rel_primal = h_rel_p_[b];
+            r.rel_dual = h_rel_d_[b];
+            r.rel_gap = h_rel_gap_[b];
+            r.last_metric = h_kkt_[b];
+            r.solve_seconds = secs;
+            r.iterate_seconds = ms * 1e-3;
+            r.fp32_iterations = std::min<long long>(fp32_iters, h_iters_[b]);
+            r.kernel_launches = launches;
+            r.primal_residual = r.stationarity_residual = r.complementarity_residual =
+                std::numeric_limits<double>::quiet_NaN();
+            r.message[0] = '\0';
+        }
+    }
+
+private:
+    bool over_time(std::chrono::steady_clock::time_point t0) const {
+        return std::isfinite(o_.time_limit_seconds) && seconds_since(t0) >= o_.time_limit_seconds;
+    }
+
+    void concatenate(const vk_problem *probs) {
+        row_off_.assign(B_ + 1, 0);
+        col_off_.assign(B_ + 1, 0);
+        std::vector<int64_t> nnz_off(B_ + 1, 0);
+        for (int b = 0; b < B_; ++b) {
+            const vk_problem &p = probs[b];
+            row_off_[b + 1] = row_off_[b] + static_cast<int>(p.A.rows);
+            col_off_[b + 1] = col_off_[b] + static_cast<int>(p.A.cols);
+            nnz_off[b + 1] = nnz_off[b] + (p.A.rows > 0 ? p.A.row_offsets[p.A.rows] : 0);
+        }
+        m_ = row_off_[B_];
+        n_ = col_off_[B_];
+        nnz_ = nnz_off[B_];
+        h_ro_.assign(m_ + 1, 0);
+        h_ci_.resize(nnz_);
+        h_v_.resize(nnz_);
+        h_c_.resize(n_);
+        h_vl_.resize(n_);
+        h_vu_.resize(n_);
+        h_rl_.resize(m_);
+        h_ru_.resize(m_);
+        offset_.resize(B_);
+        h_rinst_.resize(m_);
+        h_cinst_.resize(n_);
+        for (int b = 0; b < B_; ++b) {
+            const vk_problem &p = probs[b];
+            const int r0 = row_off_[b], c0 = col_off_[b];
+            const int64_t k0 = nnz_off[b];
+            for (int64_t i = 0; i < p.A.rows; ++i) {
+                h_ro_[r0 + i + 1] = k0 + p.A.row_offsets[i + 1];
+                h_rinst_[r0 + i] = b;
+                h_rl_[r0 + i] = p.row_lower[i];
+                h_ru_[r0 + i] = p.row_upper[i];
+            }
+            const int64_t nz = nnz_off[b + 1] - k0;
+            for (int64_t k = 0; k < nz; ++k) {
+                h_ci_[k0 + k] = c0 + p.A.col_indices[k];
+                h_v_[k0 + k] = p.A.values[k];
+            }
+            for (int64_t j = 0; j < p.A.cols; ++j) {
+                h_c_[c0 + j] = p.c[j];
+                h_vl_[c0 + j] = p.var_lower[j];
+                h_vu_[c0 + j] = p.var_upper[j];
+                h_cinst_[c0 + j] = b;
+            }
+            offset_[b] = p.objective_offset;
+        }
+        // norms in original units per instance
+        bnorm_.assign(B_, 0.0);
+        cnorm_.assign(B_, 0.0);
+        for (int b = 0; b < B_; ++b) {
+            double c2 = 0.0, b2 = 0.0;
+            for (int j = col_off_[b]; j < col_off_[b + 1]; ++j) c2 += h_c_[j] * h_c_[j];
+            for (int i = row_off_[b]; i < row_off_[b + 1]; ++i) {
+                double v = 0.0;
+                if (std::isfinite(h_rl_[i])) v = std::max(v, std::abs(h_rl_[i]));
+                if (std::isfinite(h_ru_[i])) v = std::max(v, std::abs(h_ru_[i]));
+                b2 += v * v;
+            }
+            cnorm_[b] = std::sqrt(c2);
+            bnorm_[b] = std::sqrt(b2);
+        }
+    }
+
+    template <class V>
+    void up(DevBuf<V> &d, const std::vector<V> &h) {
+        d.reset(h.empty() ? 1 : h.size());
+        if (!h.empty()) VK_CUDA(cudaMemcpyAsync(d.get(), h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice, s_));
+    }
+
+    void setup_device() {
+        // pattern with tile breaks at instance starts
+        std::vector<unsigned char> rbreak(m_ + 1, 0), cbreak(n_ + 1, 0);
+        for (int b = 0; b <= B_; ++b) {
+            rbreak[row_off_[b]] = 1;
+            cbreak[col_off_[b]] = 1;
+        }
+        DevBuf<unsigned char> drb, dcb;
+        up(drb, rbreak);
+        up(dcb, cbreak);
+        upload_pattern(m_, n_, h_ro_.data(), h_ci_.data(), a_, s_);
+        build_tiles(a_, s_, drb.get());
+        DevBuf<double> a_val;
+        a_val.reset(padded(nnz_));
+        if (nnz_ > 0) VK_CUDA(cudaMemcpyAsync(a_val.get(), h_v_.data(), nnz_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+        transpose_pattern(a_, at_, perm_, s_);
+        build_tiles(at_, s_, dcb.get());
+        DevBuf<double> at_val(padded(nnz_));
+        gather_values<double, double>(perm_.get(), a_val.get(), at_val.get(), nnz_, s_);
+        autotune_pattern<double>(a_, a_val.get(), s_);
+        autotune_pattern<double>(at_, at_val.get(), s_);
+        up(rinst_, h_rinst_);
+        up(cinst_, h_cinst_);
+        // instance of each tile and each instance's first tile
+        tile_instances(a_, h_rinst_, tinst_a_, tbeg_a_);
+        tile_instances(at_, h_cinst_, tinst_at_, tbeg_at_);
+        DevBuf<double> c, vl, vu, rl, ru;
+        up(c, h_c_);
+        up(vl, h_vl_);
+        up(vu, h_vu_);
+        up(rl, h_rl_);
+        up(ru, h_ru_);
+        // Ruiz + Pock-Chambolle, per instance by construction (block-diagonal)
+        rs_.reset(m_ > 0 ? m_ : 1);
+        cs_.reset(n_);
+        {
+            std::vector<double> one_m(m_ > 0 ? m_ : 1, 1.0), one_n(n_, 1.0);
+            VK_CUDA(cudaMemcpyAsync(rs_.get(), one_m.data(), one_m.size() * 8, cudaMemcpyHostToDevice, s_));
+            VK_CUDA(cudaMemcpyAsync(cs_.get(), one_n.data(), one_n.size() * 8, cudaMemcpyHostToDevice, s_));
+            VK_CUDA(cudaStreamSynchronize(s_));
+        }
+        if (nnz_ > 0) {
+            DevBuf<double> rn(m_), cn(n_);
+            for (int pass = 0; pass <= kRuizB; ++pass) {
+                const int mode = pass < kRuizB ? 0 : 1;
+                bscaled_norm_kernel<<<ceil_div(int64_t(m_) * 32, 256), 256, 0, s_>>>(
+                    a_.ro.get(), a_.ci.get(), a_val.get(), rs_.get(), cs_.get(), m_, mode, rn.get());
+                bscaled_norm_kernel<<<ceil_div(int64_t(n_) * 32, 256), 256, 0, s_>>>(
+                    at_.ro.get(), at_.ci.get(), at_val.get(), cs_.get(), rs_.get(), n_, mode, cn.get());
+                VK_LAUNCH_CHECK();
+                brescale_kernel<<<grid1d(m_), 256, 0, s_>>>(rs_.get(), rn.get(), m_);
+                brescale_kernel<<<grid1d(n_), 256, 0, s_>>>(cs_.get(), cn.get(), n_);
+                VK_LAUNCH_CHECK();
+            }
+        }
+        setup_state(s64_, a_val, at_val, c, rl, ru);
+        if (mixed_) setup_state(s32_, a_val, at_val, c, rl, ru);
+        // model bounds, scaled, into the float64 state (the float32 copy is made per solve)
+        bscale_vec_kernel<double><<<grid1d(n_), 256, 0, s_>>>(vl.get(), cs_.get(), n_, 1, s64_.l.get());
+        bscale_vec_kernel<double><<<grid1d(n_), 256, 0, s_>>>(vu.get(), cs_.get(), n_, 1, s64_.u.get());
+        VK_LAUNCH_CHECK();
+        step_sizes();
+        // control arrays
+        const size_t Bs = static_cast<size_t>(B_);
+        for (DevBuf<double> *d : {&eta_, &omega_, &tau_, &sigma_, &rr_, &rp_, &bn_, &cn_, &off_, &kkt_, &relp_, &reld_,
+                                  &relg_})
+            d->reset(Bs);
+        for (DevBuf<long long> *d : {&kb_, &it_, &rst_}) d->reset(Bs);
+        for (DevBuf<int> *d : {&done_, &status_, &rnow_}) d->reset(Bs);
+        VK_CUDA(cudaMemcpyAsync(bn_.get(), bnorm_.data(), Bs * 8, cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaMemcpyAsync(cn_.get(), cnorm_.data(), Bs * 8, cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaMemcpyAsync(off_.get(), offset_.data(), Bs * 8, cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaMemcpyAsync(eta_.get(), h_eta_.data(), Bs * 8, cudaMemcpyHostToDevice, s_));
+        pc_.reset(static_cast<size_t>(std::max(at_.ntiles, 1)) * 2);
+        pr_.reset(static_cast<size_t>(std::max(a_.ntiles, 1)) * 2);
+        pkr_.reset(static_cast<size_t>(std::max(a_.ntiles, 1)) * 3);
+        pkc_.reset(static_cast<size_t>(std::max(at_.ntiles, 1)) * 4);
+        sc_.reset(Bs * 2);
+        sr_.reset(Bs * 2);
+        skr_.reset(Bs * 3);
+        skc_.reset(Bs * 4);
+        for (DevBuf<double> *d : {&pc_, &pr_, &pkr_, &pkc_, &sc_, &sr_, &skr_, &skc_})
+            VK_CUDA(cudaMemsetAsync(d->get(), 0, d->bytes(), s_));
+        h_done_.resize(B_);
+        h_status_.resize(B_);
+        h_iters_.resize(B_);
+        h_restarts_.resize(B_);
+        h_kkt_.resize(B_);
+        h_rel_p_.resize(B_);
+        h_rel_d_.resize(B_);
+        h_rel_gap_.resize(B_);
+        VK_CUDA(cudaStreamSynchronize(s_));
+    }
+
+    void tile_instances(const CsrPattern32 &p, const std::vector<int> &inst, DevBuf<int> &tinst, DevBuf<int> &tbeg) {
+        std::vector<int> tiles(p.ntiles + 1);
+        VK_CUDA(cudaMemcpyAsync(tiles.data(), p.tiles.get(), tiles.size() * sizeof(int), cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaStreamSynchronize(s_));
+        std::vector<int> ti(std::max(p.ntiles, 1), 0), beg(B_ + 1, p.ntiles);
+        for (int t = p.ntiles - 1; t >= 0; --t) {
+            ti[t] = inst[tiles[t]];
+            beg[ti[t]] = t;
+        }
+        // instances without tiles start where the next instance starts
+        for (int b = B_ - 1; b >= 0; --b)
+            if (beg[b] > beg[b + 1]) beg[b] = beg[b + 1];
+        up(tinst, ti);
+        up(tbeg, beg);
+    }
+
+    template <class T>
+    void setup_state(BState<T> &st, const DevBuf<double> &a_val, const DevBuf<double> &at_val, const DevBuf<double> &c,
+                     const DevBuf<double> &rl, const DevBuf<double> &ru) {
+        const int m = m_, n = n_, mm = m > 0 ? m : 1;
+        st.ka.reset(padded(nnz_));
+        st.kat.reset(padded(nnz_));
+        if (m > 0)
+            bscale_matrix_kernel<T><<<ceil_div(int64_t(m) * 32, 256), 256, 0, s_>>>(
+                a_.ro.get(), a_.ci.get(), a_val.get(), rs_.get(), cs_.get(), m, false, st.ka.get());
+        bscale_matrix_kernel<T><<<ceil_div(int64_t(n) * 32, 256), 256, 0, s_>>>(
+            at_.ro.get(), at_.ci.get(), at_val.get(), rs_.get(), cs_.get(), n, true, st.kat.get());
+        for (DevBuf<T> *b : {&st.c, &st.l, &st.u, &st.cs, &st.x, &st.x0, &st.xbar, &st.xhat}) b->reset(n);
+        for (DevBuf<T> *b : {&st.rl, &st.ru, &st.rs, &st.y, &st.y0, &st.yhat}) b->reset(mm);
+        bscale_vec_kernel<T><<<grid1d(n), 256, 0, s_>>>(c.get(), cs_.get(), n, 0, st.c.get());
+        bconvert_kernel<T, double><<<grid1d(n), 256, 0, s_>>>(cs_.get(), n, st.cs.get());
+        VK_CUDA(cudaMemsetAsync(st.xhat.get(), 0, n * sizeof(T), s_));
+        if (m > 0) {
+            bscale_vec_kernel<T><<<grid1d(m), 256, 0, s_>>>(rl.get(), rs_.get(), m, 2, st.rl.get());
+            bscale_vec_kernel<T><<<grid1d(m), 256, 0, s_>>>(ru.get(), rs_.get(), m, 2, st.ru.get());
+            bconvert_kernel<T, double><<<grid1d(m), 256, 0, s_>>>(rs_.get(), m, st.rs.get());
+            VK_CUDA(cudaMemsetAsync(st.yhat.get(), 0, m * sizeof(T), s_));
+        }
+        VK_LAUNCH_CHECK();
+    }
+
+    // Per-instance power iteration (segment norms), omega_0 per instance.
+    void step_sizes() {
+        const int n = n_, m = m_;
+        DevBuf<double> v(n), w(m > 0 ? m : 1), z(n), nrm(B_);
+        DevBuf<int> coff;
+        up(coff, col_off_);
+        bseed_kernel<<<grid1d(n), 256, 0, s_>>>(v.get(), cinst_.get(), coff.get(), n);
+        VK_LAUNCH_CHECK();
+        const int wb = ceil_div(int64_t(B_) * 32, 256);
+        segment_norm2_kernel<double><<<wb, 256, 0, s_>>>(v.get(), coff.get(), B_, nrm.get());
+        segment_scale_kernel<double><<<grid1d(n), 256, 0, s_>>>(v.get(), cinst_.get(), n, nrm.get());
+        // Each instance keeps the estimate of the iteration at which its own
+        // sequence settled (the single-instance stopping rule); the shared
+        // loop runs until every instance has settled.
+        std::vector<double> est(B_, 0.0), prev(B_, 0.0), h(B_);
+        std::vector<char> settled(B_, 0);
+        if (nnz_ > 0 && m > 0) {
+            for (int it = 0; it < 200; ++it) {
+                BStore<double> ew;
+                ew.y = w.get();
+                launch_tiles<double, double, 1, false>(view(a_, s64_.ka.get()), Gathers<double, 1>{{v.get()}}, ew, s_);
+                BStore<double> ez;
+                ez.y = z.get();
+                launch_tiles<double, double, 1, false>(view(at_, s64_.kat.get()), Gathers<double, 1>{{w.get()}}, ez, s_);
+                segment_norm2_kernel<double><<<wb, 256, 0, s_>>>(z.get(), coff.get(), B_, nrm.get());
+                VK_CUDA(cudaMemcpyAsync(h.data(), nrm.get(), B_ * 8, cudaMemcpyDeviceToHost, s_));
+                VK_CUDA(cudaStreamSynchronize(s_));
+                segment_scale_kernel<double><<<grid1d(n), 256, 0, s_>>>(z.get(), cinst_.get(), n, nrm.get());
+                std::swap(v, z);
+                bool all = true;
+                for (int b = 0; b < B_; ++b) {
+                    if (settled[b]) continue;
+                    const double e = std::sqrt(std::sqrt(h[b]));
+                    if (it > 10 && std::abs(e - prev[b]) <= 1e-6 * e) settled[b] = 1;
+                    else all = false;
+                    prev[b] = e;
+                    est[b] = e;
+                }
+                if (all) break;
+            }
+        }
+        h_eta_.resize(B_);
+        for (int b = 0; b < B_; ++b) h_eta_[b] = est[b] > 0.0 ? 0.99 / est[b] : 1.0;
+        // omega_0 = |c^_b| / |b^_b| (scaled)
+        std::vector<double> hcs(n), hrs(m);
+        VK_CUDA(cudaMemcpyAsync(hcs.data(), cs_.get(), n * 8, cudaMemcpyDeviceToHost, s_));
+        if (m > 0) VK_CUDA(cudaMemcpyAsync(hrs.data(), rs_.get(), m * 8, cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaStreamSynchronize(s_));
+        h_omega0_.assign(B_, 1.0);
+        for (int b = 0; b < B_; ++b) {
+            double cs2 = 0.0, bs2 = 0.0;
+            for (int j = col_off_[b]; j < col_off_[b + 1]; ++j) cs2 += (h_c_[j] * hcs[j]) * (h_c_[j] * hcs[j]);
+            for (int i = row_off_[b]; i < row_off_[b + 1]; ++i) {
+                double v2 = 0.0;
+                if (std::isfinite(h_rl_[i])) v2 = std::max(v2, std::abs(h_rl_[i]));
+                if (std::isfinite(h_ru_[i])) v2 = std::max(v2, std::abs(h_ru_[i]));
+                bs2 += (v2 * hrs[i]) * (v2 * hrs[i]);
+            }
+            if (cs2 > 1e-20 && bs2 > 1e-20) h_omega0_[b] = std::sqrt(cs2) / std::sqrt(bs2);
+        }
+    }
+
+    BCtl ctl() {
+        BCtl c{};
+        c.eta = eta_.get();
+        c.omega = omega_.get();
+        c.tau = tau_.get();
+        c.sigma = sigma_.get();
+        c.r_restart = rr_.get();
+        c.r_prev = rp_.get();
+        c.bnorm = bn_.get();
+        c.cnorm = cn_.get();
+        c.offset = off_.get();
+        c.kkt = kkt_.get();
+        c.rel_p = relp_.get();
+        c.rel_d = reld_.get();
+        c.rel_gap = relg_.get();
+        c.k_base = kb_.get();
+        c.iters = it_.get();
+        c.restarts = rst_.get();
+        c.done = done_.get();
+        c.status = status_.get();
+        c.restart_now = rnow_.get();
+        c.tol = o_.relative_tolerance;
+        c.limit = o_.iteration_limit;
+        c.count = B_;
+        return c;
+    }
+
+    void reset_control() {
+        const size_t Bs = B_;
+        std::vector<double> tau(Bs), sigma(Bs), neg(Bs, -1.0), inf(Bs, std::numeric_limits<double>::infinity());
+        for (int b = 0; b < B_; ++b) {
+            tau[b] = h_eta_[b] / h_omega0_[b];
+            sigma[b] = h_eta_[b] * h_omega0_[b];
+        }
+        VK_CUDA(cudaMemcpyAsync(omega_.get(), h_omega0_.data(), Bs * 8, cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaMemcpyAsync(tau_.get(), tau.data(), Bs * 8, cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaMemcpyAsync(sigma_.get(), sigma.data(), Bs * 8, cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaMemcpyAsync(rr_.get(), neg.data(), Bs * 8, cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaMemcpyAsync(rp_.get(), inf.data(), Bs * 8, cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaMemcpyAsync(kkt_.get(), inf.data(), Bs * 8, cudaMemcpyHostToDevice, s_));
+        for (DevBuf<long long> *d : {&kb_, &it_, &rst_}) VK_CUDA(cudaMemsetAsync(d->get(), 0, d->bytes(), s_));
+        for (DevBuf<int> *d : {&done_, &status_, &rnow_}) VK_CUDA(cudaMemsetAsync(d->get(), 0, d->bytes(), s_));
+        // cold start: x = clamp(0, l, u), y = 0
+        start_kernel_launch();
+        VK_CUDA(cudaStreamSynchronize(s_));
+    }
+
+    void start_kernel_launch();
+
+    void reopen_after_fp32() {
+        read_control();
+        std::vector<int> done(B_), status(B_);
+        for (int b = 0; b < B_; ++b) {
+            const bool keep = h_status_[b] == VK_STATUS_NUMERICAL_FAILURE;
+            done[b] = keep ? 1 : 0;
+            status[b] = keep ? h_status_[b] : VK_STATUS_NOT_SOLVED;
+        }
+        VK_CUDA(cudaMemcpyAsync(done_.get(), done.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaMemcpyAsync(status_.get(), status.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaStreamSynchronize(s_));
+    }
+
+    void read_control() {
+        VK_CUDA(cudaMemcpyAsync(h_done_.data(), done_.get(), B_ * sizeof(int), cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaMemcpyAsync(h_status_.data(), status_.get(), B_ * sizeof(int), cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaMemcpyAsync(h_iters_.data(), it_.get(), B_ * sizeof(long long), cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaMemcpyAsync(h_restarts_.data(), rst_.get(), B_ * sizeof(long long), cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaMemcpyAsync(h_kkt_.data(), kkt_.get(), B_ * 8, cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaMemcpyAsync(h_rel_p_.data(), relp_.get(), B_ * 8, cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaMemcpyAsync(h_rel_d_.data(), reld_.get(), B_ * 8, cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaMemcpyAsync(h_rel_gap_.data(), relg_.get(), B_ * 8, cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaStreamSynchronize(s_));
+    }
+
+    template <class TD, class TS>
+    void copy_state(const BState<TS> &a, BState<TD> &b, bool bounds) {
+        const int m = m_, n = n_;
+        for (auto pr : {std::make_pair(&a.x, &b.x), std::make_pair(&a.x0, &b.x0), std::make_pair(&a.xhat, &b.xhat)})
+            bconvert_kernel<TD, TS><<<grid1d(n), 256, 0, s_>>>(pr.first->get(), n, pr.second->get());
+        if (bounds) {
+            bconvert_kernel<TD, TS><<<grid1d(n), 256, 0, s_>>>(a.l.get(), n, b.l.get());
+            bconvert_kernel<TD, TS><<<grid1d(n), 256, 0, s_>>>(a.u.get(), n, b.u.get());
+        }
+        if (m > 0)
+            for (auto pr : {std::make_pair(&a.y, &b.y), std::make_pair(&a.y0, &b.y0), std::make_pair(&a.yhat, &b.yhat)})
+                bconvert_kernel<TD, TS><<<grid1d(m), 256, 0, s_>>>(pr.first->get(), m, pr.second->get());
+        VK_LAUNCH_CHECK();
+    }
+
+    template <class T>
+    cudaGraphExec_t capture(BState<T> &st) {
+        VK_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+        const BCtl c = ctl();
+        for (int it = 0; it < chunk_; ++it) {
+            const bool check = it == chunk_ - 1;
+            if (check) {
+                pass_col<T, true>(st, c, it);
+                pass_row<T, true>(st, c, it);
+                kkt(st, c);
+                const int wb = ceil_div(int64_t(B_) * 32, 256);
+                segment_reduce_kernel<<<wb, 256, 0, s_>>>(pc_.get(), tbeg_at_.get(), B_, 2, sc_.get());
+                segment_reduce_kernel<<<wb, 256, 0, s_>>>(pr_.get(), tbeg_a_.get(), B_, 2, sr_.get());
+                segment_reduce_kernel<<<wb, 256, 0, s_>>>(pkr_.get(), tbeg_a_.get(), B_, 3, skr_.get());
+                segment_reduce_kernel<<<wb, 256, 0, s_>>>(pkc_.get(), tbeg_at_.get(), B_, 4, skc_.get());
+                batch_control_kernel<<<ceil_div(B_, 128), 128, 0, s_>>>(c, sc_.get(), sr_.get(), skr_.get(),
+                                                                        skc_.get(), chunk_);
+                brestart_kernel<T><<<grid1d(std::max(m_, n_)), 256, 0, s_>>>(
+                    c, cinst_.get(), rinst_.get(), st.x.get(), st.x0.get(), st.xhat.get(), n_, st.y.get(), st.y0.get(),
+                    st.yhat.get(), m_);
+                VK_LAUNCH_CHECK();
+            } else {
+                pass_col<T, false>(st, c, it);
+                pass_row<T, false>(st, c, it);
+            }
+        }
+        cudaGraph_t g;
+        VK_CUDA(cudaStreamEndCapture(s_, &g));
+        size_t nodes = 0;
+        VK_CUDA(cudaGraphGetNodes(g, nullptr, &nodes));
+        nodes_ = static_cast<long long>(nodes);
+        cudaGraphExec_t ex;
+        VK_CUDA(cudaGraphInstantiate(&ex, g, 0));
+        cudaGraphDestroy(g);
+        return ex;
+    }
+
+    template <class T, bool CHECK>
+    void pass_col(BState<T> &st, const BCtl &c, int it) {
+        BColEpi<T, CHECK> e;
+        e.ctl = c;
+        e.it = it;
+        e.inst = cinst_.get();
+        e.tile_inst = tinst_at_.get();
+        e.x = st.x.get();
+        e.xbar = st.xbar.get();
+        e.xhat = st.xhat.get();
+        e.x0 = st.x0.get();
+        e.c = st.c.get();
+        e.l = st.l.get();
+        e.u = st.u.get();
+        e.partials = pc_.get();
+        const T *yg = m_ > 0 ? st.y.get() : st.x.get();
+        launch_tiles<T, T, 1, false>(view(at_, st.kat.get()), Gathers<T, 1>{{yg}}, e, s_);
+    }
+
+    template <class T, bool CHECK>
+    void pass_row(BState<T> &st, const BCtl &c, int it) {
+        if (m_ == 0) return;
+        BRowEpi<T, CHECK> e;
+        e.ctl = c;
+        e.it = it;
+        e.inst = rinst_.get();
+        e.tile_inst = tinst_a_.get();
+        e.y = st.y.get();
+        e.yhat = st.yhat.get();
+        e.y0 = st.y0.get();
+        e.rl = st.rl.get();
+        e.ru = st.ru.get();
+        e.partials = pr_.get();
+        launch_tiles<T, T, 1, false>(view(a_, st.ka.get()), Gathers<T, 1>{{st.xbar.get()}}, e, s_);
+    }
+
+    template <class T>
+    void kkt(BState<T> &st, const BCtl &c) {
+        if (m_ > 0) {
+            BKktRowEpi<T> r;
+            r.ctl = c;
+            r.tile_inst = tinst_a_.get();
+            r.yhat = st.yhat.get();
+            r.rl = st.rl.get();
+            r.ru = st.ru.get();
+            r.rs = st.rs.get();
+            r.partials = pkr_.get();
+            launch_tiles<T, T, 1, false>(view(a_, st.ka.get()), Gathers<T, 1>{{st.xhat.get()}}, r, s_);
+        }
+        BKktColEpi<T> k;
+        k.ctl = c;
+        k.tile_inst = tinst_at_.get();
+        k.xhat = st.xhat.get();
+        k.c = st.c.get();
+        k.l = st.l.get();
+        k.u = st.u.get();
+        k.cs = st.cs.get();
+        k.partials = pkc_.get();
+        const T *yg = m_ > 0 ? st.yhat.get() : st.xhat.get();
+        launch_tiles<T, T, 1, false>(view(at_, st.kat.get()), Gathers<T, 1>{{yg}}, k, s_);
+    }
+
+    vk_options o_;
+    int B_;
+    cudaStream_t s_ = nullptr;
+    bool mixed_ = false;
+    int chunk_ = 64;
+    int m_ = 0, n_ = 0;
+    int64_t nnz_ = 0;
+    std::vector<int> row_off_, col_off_, h_rinst_, h_cinst_;
+    std::vector<int64_t> h_ro_, h_ci_;
+    std::vector<double> h_v_, h_c_, h_vl_, h_vu_, h_rl_, h_ru_, offset_, bnorm_, cnorm_, h_eta_, h_omega0_;
+    CsrPattern32 a_, at_;
+    DevBuf<int> perm_, rinst_, cinst_, tinst_a_, tinst_at_, tbeg_a_, tbeg_at_;
+    DevBuf<double> rs_, cs_;
+    BState<double> s64_;
+    BState<float> s32_;
+    DevBuf<double> eta_, omega_, tau_, sigma_, rr_, rp_, bn_, cn_, off_, kkt_, relp_, reld_, relg_;
+    DevBuf<long long> kb_, it_, rst_;
+    DevBuf<int> done_, status_, rnow_;
+    DevBuf<double> pc_, pr_, pkr_, pkc_, sc_, sr_, skr_, skc_;
+    std::vector<int> h_done_, h_status_;
+    std::vector<long long> h_iters_, h_restarts_;
+    std::vector<double> h_kkt_, h_rel_p_, h_rel_d_, h_rel_gap_;
+    cudaGraphExec_t g64_ = nullptr, g32_ = nullptr;
+    long long nodes_ = 0;
+};
+
+__global__ void bstart_kernel(const double *__restrict__ l, const double *__restrict__ u, int n, double *__restrict__ x,
+                              double *__restrict__ x0) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) {
+        const double v = clampbox(0.0, l[j], u[j]);
+        x[j] = v;
+        x0[j] = v;
+    }
+}
+
+void BatchEngine::start_kernel_launch() {
+    bstart_kernel<<<grid1d(n_), 256, 0, s_>>>(s64_.l.get(), s64_.u.get(), n_, s64_.x.get(), s64_.x0.get());
+    VK_LAUNCH_CHECK();
+    if (m_ > 0) {
+        VK_CUDA(cudaMemsetAsync(s64_.y.get(), 0, m_ * sizeof(double), s_));
+        VK_CUDA(cudaMemsetAsync(s64_.y0.get(), 0, m_ * sizeof(double), s_));
+    }
+}
+
+} // namespace
+
+// Validates every instance (LP only) and runs the batch.
+void batch_solve(const vk_problem *probs, int count, const vk_options &o, vk_result *results) {
+    if (count <= 0) throw InvalidInput("count must be positive");
+    if (o.algorithm != VK_ALGO_HALPERN) throw Unsupported("batched solves use VK_ALGO_HALPERN");
+    int64_t m = 0, n = 0, nnz = 0;
+    for (int b = 0; b < count; ++b) {
+        bool unsupported = false;
+        const std::string msg = validate_problem(probs[b], o, unsupported);
+        if (!msg.empty()) {
+            const std::string full = "instance " + std::to_string(b) + ": " + msg;
+            if (unsupported) throw Unsupported(full);
+            throw InvalidInput(full);
+        }
+        if (probs[b].Q.rows > 0 && probs[b].Q.row_offsets && probs[b].Q.row_offsets[probs[b].Q.rows] > 0)
+            throw Unsupported("instance " + std::to_string(b) + ": batched solves take LPs");
+        m += probs[b].A.rows;
+        n += probs[b].A.cols;
+        nnz += probs[b].A.rows > 0 ? probs[b].A.row_offsets[probs[b].A.rows] : 0;
+    }
+    if (m >= (int64_t(1) << 31) || n >= (int64_t(1) << 31) || nnz >= (int64_t(1) << 31))
+        throw Unsupported("the batch exceeds the int32 index range of the device structures");
+    BatchEngine eng(probs, count, o);
+    eng.solve(results);
+}
+
+} // namespace vk

@@ -360,4 +360,19 @@ void vk_spmat_destroy(vk_spmat *m) {
     }
 }
 
+int vk_batch_solve(const vk_problem *problems, int32_t count, const vk_options *opts, vk_result *results) {
+    return guarded([&] {
+        if (!problems || !results || count <= 0) return set_error(VK_ERR_INVALID, "invalid argument");
+        vk_options o;
+        if (opts)
+            o = *opts;
+        else {
+            vk_default_options(&o);
+            o.algorithm = VK_ALGO_HALPERN;
+        }
+        vk::batch_solve(problems, count, o, results);
+        return VK_OK;
+    });
+}
+
 } // extern "C"

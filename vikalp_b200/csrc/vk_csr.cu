@@ -18,11 +18,12 @@ __global__ void narrow_kernel(const int64_t *__restrict__ src, int *__restrict__
 }
 
 // flags[r] = 1 where a tile starts at row r (r == rows marks the end).
-__global__ void tile_flags_kernel(const int *__restrict__ ro, int rows, int *__restrict__ flags) {
+__global__ void tile_flags_kernel(const int *__restrict__ ro, int rows, const unsigned char *__restrict__ breaks,
+                                  int *__restrict__ flags) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r > rows) return;
     int f;
-    if (r == 0 || r == rows) {
+    if (r == 0 || r == rows || (breaks && breaks[r])) {
         f = 1;
     } else {
         const int a = ro[r - 1], b = ro[r], c = ro[r + 1];
@@ -123,10 +124,10 @@ void check_device_error(cudaStream_t s) {
     }
 }
 
-void build_tiles(CsrPattern32 &p, cudaStream_t s) {
+void build_tiles(CsrPattern32 &p, cudaStream_t s, const unsigned char *breaks) {
     const int rows = p.rows;
     DevBuf<int> flags(rows + 1), idx(rows + 1);
-    tile_flags_kernel<<<ceil_div(rows + 1, 256), 256, 0, s>>>(p.ro.get(), rows, flags.get());
+    tile_flags_kernel<<<ceil_div(rows + 1, 256), 256, 0, s>>>(p.ro.get(), rows, breaks, flags.get());
     VK_LAUNCH_CHECK();
     size_t tb = 0;
     VK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flags.get(), idx.get(), rows + 1, s));

@@ -146,7 +146,20 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     uint8_t *lrows = s_rows[warp];
     Pre *lpre = s_pre[warp];
 
+    // Per-tile reduction (opt-in): the warp's sums of this tile go to
+    // epi.tile_done and start again from zero.
+    auto after_tile = [&](int tile) {
+        if constexpr (Epi::kPerTile) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) red[r] = warp_sum(red[r]);
+            if (lane == 0) epi.tile_done(tile, red);
+#pragma unroll
+            for (int r = 0; r < NR; ++r) red[r] = 0.0;
+        }
+    };
+
     for (int tile = blockIdx.x * kWarps + warp; tile < M.ntiles; tile += gridDim.x * kWarps) {
+        if (epi.skip_tile(tile)) continue;
         const int r0 = __ldg(M.tiles + tile), r1 = __ldg(M.tiles + tile + 1);
         const int k0 = __ldg(M.tile_k + tile), k1 = __ldg(M.tile_k + tile + 1);
         const int nz = k1 - k0, nrows = r1 - r0;
@@ -178,6 +191,7 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
 #pragma unroll
             for (int q = 0; q < NV; ++q) sum[q] = epi.init(r0, q) + warp_sum(part[q]);
             if (lane == 0) epi.row_pre(r0, sum, pre, red);
+            after_tile(tile);
             continue;
         }
         // The first batch's loads go out before the prologue's.
@@ -296,6 +310,7 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
             }
         }
         __syncwarp();
+        after_tile(tile);
     }
     epi.finish(red, scratch, blockIdx.x);
 }
@@ -383,12 +398,20 @@ inline int launch_tiles(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi 
 template <class A>
 struct EpiBase {
     static constexpr int NR = 1;
+    // kPerTile: after each warp-tile the warp's reductions are summed and
+    // passed to tile_done(tile, red) (FAST order only); skip_tile(tile) lets
+    // a pass leave whole tiles untouched.
+    static constexpr bool kPerTile = false;
     struct Pre {};
     __device__ Pre load(int) const { return Pre{}; }
     __device__ A init(int, int) const { return A(0); }
     __device__ A gscale(int) const { return A(1); }
     __device__ bool skip() const { return false; }
-    __device__ void finish(double (&)[1], double *, int) const {}
+    __device__ bool skip_tile(int) const { return false; }
+    template <int NR>
+    __device__ void tile_done(int, double (&)[NR]) const {}
+    template <int NR>
+    __device__ void finish(double (&)[NR], double *, int) const {}
 };
 
 // Adapter: epilogues without a prefetch implement row(i, s, red).
@@ -407,7 +430,8 @@ struct EpiRow : EpiBase<A> {
 void upload_pattern(int64_t rows, int64_t cols, const int64_t *h_ro, const int64_t *h_ci, CsrPattern32 &out,
                     cudaStream_t s);
 // Builds the tile schedule of an int32 pattern already on the device.
-void build_tiles(CsrPattern32 &p, cudaStream_t s);
+// `breaks` (device, rows+1 bytes, optional): a tile must start where breaks[r] != 0.
+void build_tiles(CsrPattern32 &p, cudaStream_t s, const unsigned char *breaks = nullptr);
 // Transposes `a` on the device by a stable radix sort of the column indices
 // (rows ascend within each column). perm[t] = source position of entry t.
 void transpose_pattern(const CsrPattern32 &a, CsrPattern32 &at, DevBuf<int> &perm, cudaStream_t s);

@@ -69,4 +69,7 @@ std::string validate_problem(const vk_problem &p, const vk_options &o, bool &uns
 // Uploads a validated problem.
 std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s);
 
+// Independent LPs solved together (vk_batch.cu); throws on invalid input.
+void batch_solve(const vk_problem *problems, int count, const vk_options &o, vk_result *results);
+
 } // namespace vk

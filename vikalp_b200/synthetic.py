@@ -236,3 +236,15 @@ def workload_large_lp(seed: int = 12345) -> Instance:
     """m=1,000,000, n=2,000,000, ~20M nnz power-law LP."""
     return lp_powerlaw(1_000_000, 2_000_000, 20_000_000, seed=seed,
                        name=f"lp m=1e6 n=2e6 nnz~20M zipf1.5 seed={seed}")
+
+
+def workload_independent_lps(count: int = 256, seed: int = 2024, m_min: int = 500, m_max: int = 20000,
+                             per_col: int = 8) -> list[Instance]:
+    """``count`` independent LPs, m log-uniform on [m_min, m_max], n = 2m,
+    ``per_col`` nonzeros per column (lp_uniform each, seeds seed+b): the
+    independent half of the batched workload (256 LPs: ~1.35M rows,
+    ~2.7M columns, ~21.7M nonzeros in expectation)."""
+    rng = np.random.default_rng(seed)
+    ms = np.exp(rng.uniform(np.log(m_min), np.log(m_max), size=count)).astype(np.int64)
+    return [lp_uniform(int(m), int(2 * m), per_col, seed=seed + b, name=f"lp m={m} n={2 * m} seed={seed + b}")
+            for b, m in enumerate(ms)]
