@@ -238,6 +238,22 @@ int vk_vec_dot_device_noalloc(const double *x_device, const double *y_device, in
  * the whole batch. */
 int vk_batch_solve(const vk_problem *problems, int32_t count, const vk_options *opts, vk_result *results);
 
+/* Solves `count` relaxations of ONE LP that differ only in their variable
+ * bounds and warm start -- the node LPs of a branch-and-bound tree -- together
+ * with VK_ALGO_HALPERN. Replaces a loop of RelaxationOracle::solve(model,
+ * lower_override, upper_override, warm_start, options) calls on one model
+ * (RelaxationOracle.hpp:17-22). lower, upper and warm are NULL (the model's
+ * bounds / a cold start) or count * n doubles, instance b at offset b * n.
+ * An instance whose overrides or warm start fail the checks of vk_pdhg_solve
+ * gets status INVALID_MODEL and its message; the others are solved. The
+ * instances share every read of the constraint matrix (the vectors of all
+ * instances are interleaved on the device); each keeps its own primal weight,
+ * restarts and stopping, so results[b] equals, up to rounding, one
+ * VK_ALGO_HALPERN solve with those overrides. Result fields as in
+ * vk_batch_solve. */
+int vk_batch_solve_shared(const vk_problem *problem, int32_t count, const double *lower, const double *upper,
+                          const double *warm, const vk_options *opts, vk_result *results);
+
 #ifdef __cplusplus
 }
 #endif

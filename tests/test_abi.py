@@ -168,3 +168,14 @@ def test_batch_requires_halpern_and_lp():
     code, msg = batch_error([M(), q])
     assert code == vk.VK_ERR_UNSUPPORTED and msg.startswith("instance 1")
     assert vk.lib().vk_batch_solve(None, 0, None, None) == vk.VK_ERR_INVALID
+
+
+def test_shared_batch_validates_the_model():
+    with pytest.raises(vk.VkError) as e:
+        vk.batch_solve_shared(M(var_lower=np.array([3.0]), var_upper=np.array([2.0])), 4)
+    assert e.value.code == vk.VK_ERR_INVALID
+    assert e.value.msg == "variable bounds contains an invalid bound at index 0"
+    with pytest.raises(vk.VkError) as e:
+        vk.batch_solve_shared(M(), 4, algorithm="reference")
+    assert e.value.code == vk.VK_ERR_UNSUPPORTED
+    assert vk.lib().vk_batch_solve_shared(None, 1, None, None, None, None, None) == vk.VK_ERR_INVALID

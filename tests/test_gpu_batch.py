@@ -109,3 +109,78 @@ def test_batch_degenerate_members(oracle):
 def test_batch_limits(members):
     outs = vk.batch_solve(members, iteration_limit=64, relative_tolerance=1e-12)
     assert all(r["status"] == "IterationLimit" and r["iterations"] == 64 for r in outs)
+
+
+# ---- relaxations of one LP that differ in variable bounds (shared A) -------------
+
+
+@pytest.fixture(scope="module")
+def node_lp():
+    inst = synthetic.lp_uniform(600, 1500, 6, seed=77)
+    lo, hi = synthetic.bnb_nodes(inst, 8, seed=3)
+    return inst, lo, hi
+
+
+def test_shared_follows_each_single_trajectory(node_lp):
+    inst, lo, hi = node_lp
+    outs = vk.batch_solve_shared(inst, len(lo), lo, hi, iteration_limit=128, relative_tolerance=0.0, check_every=64)
+    for b, got in enumerate(outs):
+        want = halpern.solve(inst, tol=0.0, iteration_limit=128, check_every=64, lower=lo[b], upper=hi[b])
+        assert got["iterations"] == want["iterations"] == 128
+        assert got["restarts"] == want["restarts"]
+        for k in ("x", "y"):
+            scale = 1.0 + np.abs(want[k]).max()
+            assert np.max(np.abs(got[k] - want[k])) <= 1e-8 * scale, (b, k)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_shared_solves_every_node(node_lp, oracle, precision):
+    inst, lo, hi = node_lp
+    outs = vk.batch_solve_shared(inst, len(lo), lo, hi, precision=precision, iteration_limit=200000,
+                                 relative_tolerance=1e-6)
+    for b, r in enumerate(outs):
+        assert r["status"] == "Optimal", (b, r["message"])
+        assert np.all(r["x"] >= lo[b] - 1e-9) and np.all(r["x"] <= hi[b] + 1e-9)
+        k = oracle.rel_kkt(inst, r["x"], r["y"], lo[b], hi[b])
+        assert max(k["rel_primal"], k["rel_dual"], k["rel_gap"]) <= KKT_TOL, (b, k)
+        ref = highs_objective(inst, lo[b], hi[b])
+        assert abs(r["objective"] - ref) <= 1e-6 * (1 + abs(ref)), b
+        if precision == "mixed":
+            assert r["fp32_iterations"] > 0
+
+
+def test_shared_wide_batch_vector_lanes(oracle):
+    # 130 nodes: 16-byte lane packs (4 float32 / 2 float64 instances per lane)
+    # and a padded instance dimension (130 -> 256)
+    inst = synthetic.lp_uniform(150, 400, 5, seed=19)
+    lo, hi = synthetic.bnb_nodes(inst, 130, seed=4)
+    outs = vk.batch_solve_shared(inst, 130, lo, hi, precision="mixed", iteration_limit=200000,
+                                 relative_tolerance=1e-6)
+    for b in list(range(0, 130, 9)) + [129]:
+        r = outs[b]
+        assert r["status"] == "Optimal", b
+        k = oracle.rel_kkt(inst, r["x"], r["y"], lo[b], hi[b])
+        assert max(k["rel_primal"], k["rel_dual"], k["rel_gap"]) <= KKT_TOL, (b, k)
+        assert abs(r["objective"] - highs_objective(inst, lo[b], hi[b])) <= 1e-6 * (1 + abs(r["objective"])), b
+    assert all(r["status"] == "Optimal" for r in outs)
+
+
+def test_shared_invalid_member_and_warm_start(node_lp):
+    inst, lo, hi = node_lp
+    lo, hi = lo.copy(), hi.copy()
+    lo[2, 5], hi[2, 5] = 3.0, 1.0
+    outs = vk.batch_solve_shared(inst, len(lo), lo, hi, iteration_limit=200000, relative_tolerance=1e-6)
+    assert outs[2]["status"] == "InvalidModel"
+    assert outs[2]["message"] == "variable bound overrides contain an invalid interval"
+    assert all(r["status"] == "Optimal" for b, r in enumerate(outs) if b != 2)
+    # warm starts (primal, as RelaxationOracle passes them): each instance
+    # follows the restatement's warm-started trajectory
+    lo[2, 5], hi[2, 5] = inst.var_lower[5], inst.var_upper[5]
+    warm = np.stack([r["x"] if b != 2 else np.zeros(inst.n) for b, r in enumerate(outs)])
+    warm += np.random.default_rng(1).uniform(-0.5, 0.5, warm.shape)
+    again = vk.batch_solve_shared(inst, len(lo), lo, hi, warm, iteration_limit=128, relative_tolerance=0.0)
+    for b in range(len(lo)):
+        want = halpern.solve(inst, tol=0.0, iteration_limit=128, lower=lo[b], upper=hi[b], warm=warm[b])
+        assert again[b]["restarts"] == want["restarts"]
+        for k in ("x", "y"):
+            assert np.max(np.abs(again[b][k] - want[k])) <= 1e-8 * (1.0 + np.abs(want[k]).max()), (b, k)

@@ -94,6 +94,8 @@ _SIGNATURES = {
     "vk_vec_norm_inf_device": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "vk_vec_dot_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "vk_batch_solve": (C.c_int, [C.POINTER(Problem), C.c_int32, C.POINTER(Options), C.POINTER(Result)]),
+    "vk_batch_solve_shared": (C.c_int, [C.POINTER(Problem), C.c_int32, _f64p, _f64p, _f64p, C.POINTER(Options),
+                                        C.POINTER(Result)]),
 }
 
 _lib = None
@@ -262,6 +264,32 @@ def batch_solve(instances, **opts) -> list[dict]:
                    objective=r.objective, rel_primal=r.rel_primal, rel_dual=r.rel_dual, rel_gap=r.rel_gap,
                    last_metric=r.last_metric, solve_seconds=r.solve_seconds, iterate_seconds=r.iterate_seconds,
                    fp32_iterations=r.fp32_iterations, kernel_launches=r.kernel_launches)
+    return outs
+
+
+def batch_solve_shared(inst, count, lower=None, upper=None, warm=None, **opts) -> list[dict]:
+    """Relaxations of one LP differing in variable bounds (vk_batch_solve_shared).
+
+    lower / upper / warm: None or arrays of shape (count, n)."""
+    opts.setdefault("algorithm", "halpern")
+    keep = _Keep()
+    p = problem_struct(inst, keep)
+    arr = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(count, inst.n)  # noqa: E731
+    lower, upper, warm = arr(lower), arr(upper), arr(warm)
+    results = (Result * count)()
+    outs = []
+    for r in results:
+        o = {"x": np.zeros(inst.n), "y": np.zeros(inst.m)}
+        r.x, r.y = _p(o["x"]), _p(o["y"])
+        outs.append(o)
+    o = options(**opts)
+    _check(lib().vk_batch_solve_shared(C.byref(p), count, keep.f(lower), keep.f(upper), keep.f(warm), C.byref(o),
+                                       results))
+    for out, r in zip(outs, results):
+        out.update(status=STATUS.get(r.status, str(r.status)), iterations=r.iterations, restarts=r.restarts,
+                   objective=r.objective, rel_primal=r.rel_primal, rel_dual=r.rel_dual, rel_gap=r.rel_gap,
+                   last_metric=r.last_metric, solve_seconds=r.solve_seconds, iterate_seconds=r.iterate_seconds,
+                   fp32_iterations=r.fp32_iterations, kernel_launches=r.kernel_launches, message=r.message.decode())
     return outs
 
 

@@ -18,6 +18,8 @@
 #include <cmath>
 #include <limits>
 #include <numeric>
+#include <string>
+#include <type_traits>
 
 namespace vk {
 namespace {
@@ -378,7 +380,11 @@ struct BState {
     DevBuf<T> ka, kat, c, l, u, rl, ru, rs, cs, x, x0, xbar, xhat, y, y0, yhat;
 };
 
+class SharedEngine;
+
 class BatchEngine {
+    friend class SharedEngine; // reuses the scaled model of a one-instance batch
+
 public:
     BatchEngine(const vk_problem *probs, int count, const vk_options &o) : o_(o), B_(count) {
         VK_CUDA(cudaSetDevice(o.device));
@@ -1000,6 +1006,922 @@ void BatchEngine::start_kernel_launch() {
     }
 }
 
+// ---- shared-A batches: relaxations of one LP that differ in variable bounds ----
+//
+// The vectors of all instances are interleaved, instance-minor: X[j * ld + b]
+// (ld = instance count rounded up to the lane width). One warp handles one
+// matrix row for a group of 32 * VEC instances, each lane VEC adjacent
+// instances, so every nonzero (column index, value: one broadcast load) pulls a
+// contiguous 16-byte slice per lane of the gathered vector: the products of all
+// instances share one read of the matrix, and the gathers are coalesced. The
+// blocks of a group all serve the same instances, so per-instance check sums
+// are reduced in registers, then across the block's warps in shared memory and
+// finally over the blocks in a fixed order (deterministic).
+
+template <class T, int VEC>
+__device__ __forceinline__ void ldg_vec(const T *p, T (&o)[VEC]) {
+    if constexpr (VEC == 1) {
+        o[0] = __ldg(p);
+    } else if constexpr (std::is_same<T, double>::value && VEC == 2) {
+        const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+        o[0] = v.x;
+        o[1] = v.y;
+    } else {
+        static_assert(std::is_same<T, float>::value && VEC == 4, "16-byte packs only");
+        const float4 v = __ldg(reinterpret_cast<const float4 *>(p));
+        o[0] = v.x;
+        o[1] = v.y;
+        o[2] = v.z;
+        o[3] = v.w;
+    }
+}
+
+template <class T, int VEC>
+__device__ __forceinline__ void ld_vec(const T *p, T (&o)[VEC]) {
+    if constexpr (VEC == 1) {
+        o[0] = *p;
+    } else if constexpr (std::is_same<T, double>::value && VEC == 2) {
+        const double2 v = *reinterpret_cast<const double2 *>(p);
+        o[0] = v.x;
+        o[1] = v.y;
+    } else {
+        const float4 v = *reinterpret_cast<const float4 *>(p);
+        o[0] = v.x;
+        o[1] = v.y;
+        o[2] = v.z;
+        o[3] = v.w;
+    }
+}
+
+// Stores the lanes' active elements: one vector store when all are active.
+template <class T, int VEC>
+__device__ __forceinline__ void st_vec(T *p, const T (&v)[VEC], const bool (&act)[VEC], bool all) {
+    if (all) {
+        if constexpr (VEC == 1) {
+            *p = v[0];
+        } else if constexpr (std::is_same<T, double>::value && VEC == 2) {
+            *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[1]);
+        } else {
+            *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < VEC; ++q)
+            if (act[q]) p[q] = v[q];
+    }
+}
+
+constexpr int kSpmmWarps = 8;
+constexpr int kSpmmMaxR = 4;
+
+// Per-lane instance state common to the epilogues.
+template <class T, int VEC>
+struct LaneBase {
+    bool act[VEC];
+    bool all;
+};
+
+template <class T, int VEC>
+__device__ __forceinline__ void lane_activity(const BCtl &c, int b0, LaneBase<T, VEC> &L) {
+    L.all = true;
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+        const int b = b0 + q;
+        L.act[q] = b < c.count && c.done[b] == 0;
+        L.all = L.all && L.act[q];
+    }
+}
+
+// Variable bounds of instance slice [b0, b0+VEC) at column j: the shared
+// scaled model bounds unless the column has an override row.
+template <class T, int VEC>
+__device__ __forceinline__ void col_bounds(int j, int b0, int ld, const T *l, const T *u, const int *ovr,
+                                           const T *ovl, const T *ovu, T (&lo)[VEC], T (&hi)[VEC]) {
+    const int o = __ldg(ovr + j);
+    if (o >= 0) {
+        ldg_vec<T, VEC>(ovl + static_cast<size_t>(o) * ld + b0, lo);
+        ldg_vec<T, VEC>(ovu + static_cast<size_t>(o) * ld + b0, hi);
+    } else {
+        const T a = __ldg(l + j), b = __ldg(u + j);
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            lo[q] = a;
+            hi[q] = b;
+        }
+    }
+}
+
+template <class T, int VEC, bool CHECK>
+struct SColEpi {
+    static constexpr int NR = CHECK ? 2 : 0;
+    BCtl ctl;
+    int it, ld;
+    T *x, *xbar, *xhat;
+    const T *x0, *c, *l, *u, *ovl, *ovu;
+    const int *ovr;
+    struct Lane : LaneBase<T, VEC> {
+        T tau[VEC], lam[VEC];
+    };
+    __device__ Lane lane(int b0) const {
+        Lane L;
+        lane_activity<T, VEC>(ctl, b0, L);
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            const int b = L.act[q] ? b0 + q : 0;
+            L.tau[q] = static_cast<T>(ctl.tau[b]);
+            L.lam[q] = static_cast<T>(lam_of(ctl, b, it));
+        }
+        return L;
+    }
+    __device__ void row(int j, int b0, const Lane &L, const T (&s)[VEC], double (&red)[kSpmmMaxR][VEC]) const {
+        const size_t at = static_cast<size_t>(j) * ld + b0;
+        T xv[VEC], x0v[VEC], lo[VEC], hi[VEC], xh[VEC], xb[VEC], xn[VEC];
+        ld_vec<T, VEC>(x + at, xv);
+        ld_vec<T, VEC>(x0 + at, x0v);
+        col_bounds<T, VEC>(j, b0, ld, l, u, ovr, ovl, ovu, lo, hi);
+        const T cj = __ldg(c + j);
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            xh[q] = clampbox(xv[q] - L.tau[q] * (cj + s[q]), lo[q], hi[q]);
+            xb[q] = T(2) * xh[q] - xv[q];
+            xn[q] = L.lam[q] * ((T(1) + T(kRhoB)) * xh[q] - T(kRhoB) * xv[q]) + (T(1) - L.lam[q]) * x0v[q];
+            if (CHECK && L.act[q]) {
+                const double d0 = static_cast<double>(xh[q]) - static_cast<double>(xv[q]);
+                const double d1 = static_cast<double>(xh[q]) - static_cast<double>(x0v[q]);
+                red[0][q] += d0 * d0;
+                red[1][q] += d1 * d1;
+            }
+        }
+        st_vec<T, VEC>(xbar + at, xb, L.act, L.all);
+        st_vec<T, VEC>(x + at, xn, L.act, L.all);
+        if (CHECK) st_vec<T, VEC>(xhat + at, xh, L.act, L.all);
+    }
+};
+
+template <class T, int VEC, bool CHECK>
+struct SRowEpi {
+    static constexpr int NR = CHECK ? 2 : 0;
+    BCtl ctl;
+    int it, ld;
+    T *y, *yhat;
+    const T *y0, *rl, *ru;
+    struct Lane : LaneBase<T, VEC> {
+        T sigma[VEC], lam[VEC];
+    };
+    __device__ Lane lane(int b0) const {
+        Lane L;
+        lane_activity<T, VEC>(ctl, b0, L);
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            const int b = L.act[q] ? b0 + q : 0;
+            L.sigma[q] = static_cast<T>(ctl.sigma[b]);
+            L.lam[q] = static_cast<T>(lam_of(ctl, b, it));
+        }
+        return L;
+    }
+    __device__ void row(int i, int b0, const Lane &L, const T (&s)[VEC], double (&red)[kSpmmMaxR][VEC]) const {
+        const size_t at = static_cast<size_t>(i) * ld + b0;
+        T yv[VEC], y0v[VEC], yh[VEC], yn[VEC];
+        ld_vec<T, VEC>(y + at, yv);
+        ld_vec<T, VEC>(y0 + at, y0v);
+        const T lo = __ldg(rl + i), hi = __ldg(ru + i);
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            const T v = yv[q] + L.sigma[q] * s[q];
+            yh[q] = v - clampbox(v, L.sigma[q] * lo, L.sigma[q] * hi);
+            yn[q] = L.lam[q] * ((T(1) + T(kRhoB)) * yh[q] - T(kRhoB) * yv[q]) + (T(1) - L.lam[q]) * y0v[q];
+            if (CHECK && L.act[q]) {
+                const double d0 = static_cast<double>(yh[q]) - static_cast<double>(yv[q]);
+                const double d1 = static_cast<double>(yh[q]) - static_cast<double>(y0v[q]);
+                red[0][q] += d0 * d0;
+                red[1][q] += d1 * d1;
+            }
+        }
+        st_vec<T, VEC>(y + at, yn, L.act, L.all);
+        if (CHECK) st_vec<T, VEC>(yhat + at, yh, L.act, L.all);
+    }
+};
+
+// Relative-KKT pieces (the single-instance definitions, per instance).
+template <class T, int VEC>
+struct SKktRowEpi {
+    static constexpr int NR = 3;
+    BCtl ctl;
+    int ld;
+    const T *yhat, *rl, *ru, *rs;
+    using Lane = LaneBase<T, VEC>;
+    __device__ Lane lane(int b0) const {
+        Lane L;
+        lane_activity<T, VEC>(ctl, b0, L);
+        return L;
+    }
+    __device__ void row(int i, int b0, const Lane &L, const T (&s)[VEC], double (&red)[kSpmmMaxR][VEC]) const {
+        T yv[VEC];
+        ld_vec<T, VEC>(yhat + static_cast<size_t>(i) * ld + b0, yv);
+        const double lo = static_cast<double>(__ldg(rl + i)), hi = static_cast<double>(__ldg(ru + i));
+        const double r = static_cast<double>(__ldg(rs + i));
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            if (!L.act[q]) continue;
+            const double a = static_cast<double>(s[q]);
+            const double pr = (a - clampbox(a, lo, hi)) / r;
+            red[0][q] += pr * pr;
+            const double y = static_cast<double>(yv[q]);
+            const double yl = smax(0.0, -y), yu = smax(0.0, y);
+            if (yl > 0.0) {
+                if (isfinite(lo)) red[1][q] += lo * yl; else red[2][q] += (r * yl) * (r * yl);
+            }
+            if (yu > 0.0) {
+                if (isfinite(hi)) red[1][q] -= hi * yu; else red[2][q] += (r * yu) * (r * yu);
+            }
+        }
+    }
+};
+
+template <class T, int VEC>
+struct SKktColEpi {
+    static constexpr int NR = 4;
+    BCtl ctl;
+    int ld;
+    const T *xhat, *c, *l, *u, *ovl, *ovu, *cs;
+    const int *ovr;
+    using Lane = LaneBase<T, VEC>;
+    __device__ Lane lane(int b0) const {
+        Lane L;
+        lane_activity<T, VEC>(ctl, b0, L);
+        return L;
+    }
+    __device__ void row(int j, int b0, const Lane &L, const T (&s)[VEC], double (&red)[kSpmmMaxR][VEC]) const {
+        T xv[VEC], lo[VEC], hi[VEC];
+        ld_vec<T, VEC>(xhat + static_cast<size_t>(j) * ld + b0, xv);
+        col_bounds<T, VEC>(j, b0, ld, l, u, ovr, ovl, ovu, lo, hi);
+        const double cj = static_cast<double>(__ldg(c + j)), d = static_cast<double>(__ldg(cs + j));
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            if (!L.act[q]) continue;
+            const double lam = cj + static_cast<double>(s[q]);
+            const double a = static_cast<double>(lo[q]), b = static_cast<double>(hi[q]);
+            const double x = static_cast<double>(xv[q]);
+            const double vl = smax(0.0, lam), vu = smax(0.0, -lam);
+            if (vl > 0.0) {
+                if (isfinite(a)) red[1][q] += a * vl; else red[0][q] += (vl / d) * (vl / d);
+            }
+            if (vu > 0.0) {
+                if (isfinite(b)) red[1][q] -= b * vu; else red[0][q] += (vu / d) * (vu / d);
+            }
+            red[2][q] += cj * x;
+            const double bx = (x - clampbox(x, a, b)) * d;
+            red[3][q] += bx * bx;
+        }
+    }
+};
+
+template <class T>
+struct SpmmMat {
+    const int *ro, *ci;
+    const T *val;
+    int rows;
+};
+
+// One pass: for every row i and instance b, s = sum_k val_k * X[ci_k * ld + b],
+// handed to the epilogue. blockIdx.x = p * G + g: group g of 32*VEC instances,
+// block p of the P blocks serving that group (rows p*8 + warp, stride P*8).
+template <class T, int VEC, class Epi>
+__global__ void __launch_bounds__(kSpmmWarps * 32, 3)
+    spmm_kernel(SpmmMat<T> M, const T *__restrict__ X, int ld, int G, Epi epi, double *__restrict__ partials) {
+    constexpr int NR = Epi::NR;
+    const int g = blockIdx.x % G, p = blockIdx.x / G, P = gridDim.x / G;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b0 = g * 32 * VEC + lane * VEC;
+    const typename Epi::Lane L = epi.lane(b0);
+    double red[kSpmmMaxR][VEC];
+#pragma unroll
+    for (int r = 0; r < kSpmmMaxR; ++r)
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) red[r][q] = 0.0;
+    const T *Xb = X + b0;
+    for (int i = p * kSpmmWarps + warp; i < M.rows; i += P * kSpmmWarps) {
+        const int k0 = __ldg(M.ro + i), k1 = __ldg(M.ro + i + 1);
+        T acc[VEC];
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) acc[q] = T(0);
+        int k = k0;
+        for (; k + 4 <= k1; k += 4) {
+            int cc[4];
+            T vv[4], xv[4][VEC];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                cc[t] = __ldg(M.ci + k + t);
+                vv[t] = __ldg(M.val + k + t);
+            }
+#pragma unroll
+            for (int t = 0; t < 4; ++t) ldg_vec<T, VEC>(Xb + static_cast<size_t>(cc[t]) * ld, xv[t]);
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) acc[q] += vv[t] * xv[t][q];
+        }
+        for (; k < k1; ++k) {
+            const int cc = __ldg(M.ci + k);
+            const T vv = __ldg(M.val + k);
+            T xv[VEC];
+            ldg_vec<T, VEC>(Xb + static_cast<size_t>(cc) * ld, xv);
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) acc[q] += vv * xv[q];
+        }
+        epi.row(i, b0, L, acc, red);
+    }
+    if constexpr (NR > 0) {
+        __shared__ double sred[kSpmmWarps][NR][32 * VEC];
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) sred[warp][r][lane * VEC + q] = red[r][q];
+        __syncthreads();
+        for (int e = threadIdx.x; e < NR * 32 * VEC; e += blockDim.x) {
+            const int r = e / (32 * VEC), t = e % (32 * VEC);
+            double acc = 0.0;
+            for (int w = 0; w < kSpmmWarps; ++w) acc += sred[w][r][t];
+            partials[(static_cast<size_t>(p) * NR + r) * ld + g * 32 * VEC + t] = acc;
+        }
+    }
+}
+
+// out[b * R + r] = sum_p partials[(p * R + r) * ld + b], p in order.
+__global__ void spmm_reduce_kernel(const double *__restrict__ partials, int P, int R, int ld, int count,
+                                   double *__restrict__ out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= count * R) return;
+    const int b = e / R, r = e % R;
+    double acc = 0.0;
+    for (int p = 0; p < P; ++p) acc += partials[(static_cast<size_t>(p) * R + r) * ld + b];
+    out[e] = acc;
+}
+
+template <class T>
+__global__ void srestart_kernel(BCtl c, int ld, T *x, T *x0, const T *xhat, int64_t nx, T *y, T *y0, const T *yhat,
+                                int64_t ny) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int b = static_cast<int>(e % ld);
+    if (b >= c.count || !c.restart_now[b] || c.done[b]) return;
+    if (e < nx) {
+        x[e] = xhat[e];
+        x0[e] = xhat[e];
+    }
+    if (e < ny) {
+        y[e] = yhat[e];
+        y0[e] = yhat[e];
+    }
+}
+
+template <class TD, class TS>
+__global__ void sconvert_kernel(const TS *__restrict__ a, int64_t n, TD *__restrict__ out) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = static_cast<TD>(a[i]);
+}
+
+// Start point per instance: clamp(warm / D or 0, bounds), interleaved.
+__global__ void sstart_kernel(const double *__restrict__ warm, const double *__restrict__ lo,
+                              const double *__restrict__ hi, const double *__restrict__ cs, int n, int count, int ld,
+                              double *__restrict__ x, double *__restrict__ x0) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= static_cast<int64_t>(n) * ld) return;
+    const int j = static_cast<int>(e / ld), b = static_cast<int>(e % ld);
+    double v = 0.0;
+    if (b < count) {
+        const size_t src = static_cast<size_t>(b) * n + j;
+        const double d = cs[j];
+        const double l = isfinite(lo[src]) ? lo[src] / d : lo[src];
+        const double u = isfinite(hi[src]) ? hi[src] / d : hi[src];
+        v = clampbox(warm ? warm[src] / d : 0.0, l, u);
+    }
+    x[e] = v;
+    x0[e] = v;
+}
+
+// Override table rows: for each overridden column, the scaled bounds of every instance.
+__global__ void soverride_kernel(const double *__restrict__ lo, const double *__restrict__ hi,
+                                 const double *__restrict__ cs, const int *__restrict__ cols, int nov, int n,
+                                 int count, int ld, double *__restrict__ ovl, double *__restrict__ ovu) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= static_cast<int64_t>(nov) * ld) return;
+    const int o = static_cast<int>(e / ld), b = static_cast<int>(e % ld);
+    double l = 0.0, u = 0.0;
+    if (b < count) {
+        const int j = cols[o];
+        const size_t src = static_cast<size_t>(b) * n + j;
+        const double d = cs[j];
+        l = isfinite(lo[src]) ? lo[src] / d : lo[src];
+        u = isfinite(hi[src]) ? hi[src] / d : hi[src];
+    }
+    ovl[e] = l;
+    ovu[e] = u;
+}
+
+// out[b * n + j] = a[j * ld + b] * s[j]: unscale and de-interleave.
+__global__ void sunscale_kernel(const double *__restrict__ a, const double *__restrict__ s, int n, int count, int ld,
+                                double *__restrict__ out) {
+    const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= static_cast<int64_t>(n) * count) return;
+    const int b = static_cast<int>(e / n), j = static_cast<int>(e % n);
+    out[e] = a[static_cast<size_t>(j) * ld + b] * s[j];
+}
+
+template <class T>
+struct SState {
+    DevBuf<T> x, x0, xbar, xhat, y, y0, yhat, l, u, ovl, ovu, c, rl, ru, rs, cs;
+};
+
+inline int grid_for64(int64_t n) { return static_cast<int>(std::max<int64_t>(1, (n + 255) / 256)); }
+
+class SharedEngine {
+public:
+    SharedEngine(const vk_problem &p, int count, const vk_options &o)
+        : o_(o), B_(count), base_(&p, 1, base_options(o)), model_(p) {
+        m_ = base_.m_;
+        n_ = base_.n_;
+        s_ = base_.s_;
+        mixed_ = o.precision == VK_PREC_MIXED;
+        chunk_ = base_.chunk_;
+        const int width = B_ >= 128 ? 128 : 32;
+        ld_ = (B_ + width - 1) / width * width;
+        vec32_ = B_ >= 128 ? 4 : 1;
+        vec64_ = (B_ >= 64 && ld_ % 64 == 0) ? 2 : 1;
+        const int sms = sm_count();
+        P32_ = std::max(1, 4 * sms / (ld_ / (32 * vec32_)));
+        P64_ = std::max(1, 4 * sms / (ld_ / (32 * vec64_)));
+        control_arrays();
+        pmax_ = std::max(P32_, P64_);
+        partial_.reset(static_cast<size_t>(pmax_) * kSpmmMaxR * ld_);
+        sc_.reset(static_cast<size_t>(B_) * 2);
+        sr_.reset(static_cast<size_t>(B_) * 2);
+        skr_.reset(static_cast<size_t>(B_) * 3);
+        skc_.reset(static_cast<size_t>(B_) * 4);
+    }
+    ~SharedEngine() {
+        if (g64_) cudaGraphExecDestroy(g64_);
+        if (g32_) cudaGraphExecDestroy(g32_);
+    }
+
+    void solve(const double *lower, const double *upper, const double *warm, vk_result *results) {
+        const auto started = std::chrono::steady_clock::now();
+        const int n = n_, m = m_;
+        // per-instance checks (continuous_common.hpp:80-110, pdhg.cpp:29-33)
+        std::vector<int> invalid(B_, 0);
+        std::vector<std::string> why(B_);
+        std::vector<char> overridden(n, 0);
+        for (int b = 0; b < B_; ++b) {
+            const size_t o = static_cast<size_t>(b) * n;
+            for (int j = 0; j < n && !invalid[b]; ++j) {
+                const double l = lower ? lower[o + j] : model_.var_lower[j];
+                const double u = upper ? upper[o + j] : model_.var_upper[j];
+                if ((lower && std::isnan(lower[o + j])) || (upper && std::isnan(upper[o + j]))) {
+                    invalid[b] = 1;
+                    why[b] = "variable bound overrides must be empty or sized and non-NaN";
+                } else if (std::isnan(l) || std::isnan(u) || l > u) {
+                    invalid[b] = 1;
+                    why[b] = "variable bound overrides contain an invalid interval";
+                } else if (warm && !std::isfinite(warm[o + j])) {
+                    invalid[b] = 1;
+                    why[b] = "warm start must be empty or finite and sized to the model";
+                }
+                if (l != model_.var_lower[j] || u != model_.var_upper[j]) overridden[j] = 1;
+            }
+        }
+        std::vector<int> ov_cols, ov_index(n, -1);
+        for (int j = 0; j < n; ++j)
+            if (overridden[j]) {
+                ov_index[j] = static_cast<int>(ov_cols.size());
+                ov_cols.push_back(j);
+            }
+        const int nov = static_cast<int>(ov_cols.size());
+        // bounds and warm start of every instance, on the device
+        const size_t bn = static_cast<size_t>(B_) * n;
+        DevBuf<double> dlo(bn), dhi(bn), dwarm(warm ? bn : 1);
+        {
+            std::vector<double> tmp;
+            for (int side = 0; side < 2; ++side) {
+                const double *src = side == 0 ? lower : upper;
+                const double *model = side == 0 ? model_.var_lower : model_.var_upper;
+                DevBuf<double> &dst = side == 0 ? dlo : dhi;
+                if (src) {
+                    VK_CUDA(cudaMemcpyAsync(dst.get(), src, bn * sizeof(double), cudaMemcpyHostToDevice, s_));
+                } else {
+                    tmp.resize(bn);
+                    for (int b = 0; b < B_; ++b) std::copy(model, model + n, tmp.begin() + static_cast<size_t>(b) * n);
+                    VK_CUDA(cudaMemcpyAsync(dst.get(), tmp.data(), bn * sizeof(double), cudaMemcpyHostToDevice, s_));
+                    VK_CUDA(cudaStreamSynchronize(s_));
+                }
+            }
+            if (warm) VK_CUDA(cudaMemcpyAsync(dwarm.get(), warm, bn * sizeof(double), cudaMemcpyHostToDevice, s_));
+        }
+        DevBuf<int> dov_index, dov_cols;
+        dov_index.reset(n);
+        VK_CUDA(cudaMemcpyAsync(dov_index.get(), ov_index.data(), n * sizeof(int), cudaMemcpyHostToDevice, s_));
+        dov_cols.reset(std::max(nov, 1));
+        if (nov > 0)
+            VK_CUDA(cudaMemcpyAsync(dov_cols.get(), ov_cols.data(), nov * sizeof(int), cudaMemcpyHostToDevice, s_));
+        // float64 state
+        alloc_state(s64_, nov);
+        state_model(s64_);
+        const int64_t nx = static_cast<int64_t>(n) * ld_, ny = static_cast<int64_t>(m) * ld_;
+        sstart_kernel<<<grid_for64(nx), 256, 0, s_>>>(warm ? dwarm.get() : nullptr, dlo.get(), dhi.get(),
+                                                      base_.cs_.get(), n, B_, ld_, s64_.x.get(), s64_.x0.get());
+        if (nov > 0)
+            soverride_kernel<<<grid_for64(static_cast<int64_t>(nov) * ld_), 256, 0, s_>>>(
+                dlo.get(), dhi.get(), base_.cs_.get(), dov_cols.get(), nov, n, B_, ld_, s64_.ovl.get(), s64_.ovu.get());
+        VK_LAUNCH_CHECK();
+        if (m > 0) {
+            VK_CUDA(cudaMemsetAsync(s64_.y.get(), 0, ny * sizeof(double), s_));
+            VK_CUDA(cudaMemsetAsync(s64_.y0.get(), 0, ny * sizeof(double), s_));
+            VK_CUDA(cudaMemsetAsync(s64_.yhat.get(), 0, ny * sizeof(double), s_));
+        }
+        VK_CUDA(cudaMemsetAsync(s64_.xhat.get(), 0, nx * sizeof(double), s_));
+        VK_CUDA(cudaMemsetAsync(s64_.xbar.get(), 0, nx * sizeof(double), s_));
+        ov_ = dov_index.get();
+        reset_control(invalid);
+
+        cudaEvent_t e0, e1;
+        VK_CUDA(cudaEventCreate(&e0));
+        VK_CUDA(cudaEventCreate(&e1));
+        VK_CUDA(cudaEventRecord(e0, s_));
+        long long launches = 0, fp32_iters = 0;
+        bool timed_out = false;
+        if (g64_) {
+            cudaGraphExecDestroy(g64_);
+            g64_ = nullptr;
+        }
+        if (g32_) {
+            cudaGraphExecDestroy(g32_);
+            g32_ = nullptr;
+        }
+        if (mixed_) {
+            alloc_state(s32_, nov);
+            state_model(s32_);
+            copy_state<float, double>(s64_, s32_, nov, true);
+            g32_ = vec32_ == 4 ? capture<float, 4>(s32_) : capture<float, 1>(s32_);
+            std::vector<double> best(B_, std::numeric_limits<double>::infinity());
+            int stall = 0;
+            for (;;) {
+                if (over_time(started)) {
+                    timed_out = true;
+                    break;
+                }
+                VK_CUDA(cudaGraphLaunch(g32_, s_));
+                launches += nodes_;
+                read_control();
+                check_device_error(s_);
+                bool improved = false, all_done = true;
+                double worst = 0.0;
+                for (int b = 0; b < B_; ++b) {
+                    if (h_done_[b]) continue;
+                    all_done = false;
+                    worst = std::max(worst, h_kkt_[b]);
+                    if (h_kkt_[b] < 0.7 * best[b]) {
+                        best[b] = h_kkt_[b];
+                        improved = true;
+                    }
+                }
+                if (all_done) break;
+                if (improved)
+                    stall = 0;
+                else if (++stall >= 6 && worst < 1e-3)
+                    break;
+            }
+            fp32_iters = h_iters_.empty() ? 0 : *std::max_element(h_iters_.begin(), h_iters_.end());
+            copy_state<double, float>(s32_, s64_, nov, false);
+            reopen(invalid);
+        }
+        if (!timed_out) {
+            g64_ = vec64_ == 2 ? capture<double, 2>(s64_) : capture<double, 1>(s64_);
+            for (;;) {
+                if (over_time(started)) {
+                    timed_out = true;
+                    break;
+                }
+                VK_CUDA(cudaGraphLaunch(g64_, s_));
+                launches += nodes_;
+                read_control();
+                check_device_error(s_);
+                if (std::all_of(h_done_.begin(), h_done_.end(), [](int d) { return d != 0; })) break;
+            }
+        }
+        VK_CUDA(cudaEventRecord(e1, s_));
+        read_control();
+        float ms = 0.f;
+        VK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        // answers (x^, y^) in original units, instance-major
+        DevBuf<double> xo(bn), yo(std::max<size_t>(1, static_cast<size_t>(B_) * m));
+        sunscale_kernel<<<grid_for64(static_cast<int64_t>(bn)), 256, 0, s_>>>(s64_.xhat.get(), base_.cs_.get(), n, B_,
+                                                                             ld_, xo.get());
+        if (m > 0)
+            sunscale_kernel<<<grid_for64(static_cast<int64_t>(B_) * m), 256, 0, s_>>>(
+                s64_.yhat.get(), base_.rs_.get(), m, B_, ld_, yo.get());
+        VK_LAUNCH_CHECK();
+        std::vector<double> hx(bn), hy(static_cast<size_t>(B_) * m);
+        VK_CUDA(cudaMemcpyAsync(hx.data(), xo.get(), bn * sizeof(double), cudaMemcpyDeviceToHost, s_));
+        if (m > 0)
+            VK_CUDA(cudaMemcpyAsync(hy.data(), yo.get(), hy.size() * sizeof(double), cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaStreamSynchronize(s_));
+        const double secs = seconds_since(started);
+        for (int b = 0; b < B_; ++b) {
+            vk_result &r = results[b];
+            r.message[0] = '\0';
+            r.primal_residual = r.stationarity_residual = r.complementarity_residual =
+                std::numeric_limits<double>::quiet_NaN();
+            r.solve_seconds = secs;
+            r.iterate_seconds = ms * 1e-3;
+            r.kernel_launches = launches;
+            if (invalid[b]) {
+                r.status = VK_STATUS_INVALID_MODEL;
+                std::snprintf(r.message, sizeof(r.message), "%s", why[b].c_str());
+                r.iterations = r.restarts = r.fp32_iterations = 0;
+                r.objective = r.rel_primal = r.rel_dual = r.rel_gap = r.last_metric =
+                    std::numeric_limits<double>::quiet_NaN();
+                continue;
+            }
+            const double *xb = hx.data() + static_cast<size_t>(b) * n;
+            if (r.x) std::copy(xb, xb + n, r.x);
+            if (r.y && m > 0) std::copy(hy.begin() + static_cast<size_t>(b) * m, hy.begin() + static_cast<size_t>(b + 1) * m, r.y);
+            double obj = model_.objective_offset;
+            for (int j = 0; j < n; ++j) obj += model_.c[j] * xb[j];
+            r.objective = obj;
+            r.status = h_done_[b] ? h_status_[b] : (timed_out ? VK_STATUS_TIME_LIMIT : VK_STATUS_ITERATION_LIMIT);
+            r.iterations = h_iters_[b];
+            r.restarts = h_restarts_[b];
+            r.rel_primal = h_rel_p_[b];
+            r.rel_dual = h_rel_d_[b];
+            r.rel_gap = h_rel_gap_[b];
+            r.last_metric = h_kkt_[b];
+            r.fp32_iterations = std::min<long long>(fp32_iters, h_iters_[b]);
+        }
+    }
+
+private:
+    static vk_options base_options(const vk_options &o) {
+        vk_options b = o;
+        b.precision = VK_PREC_MIXED; // builds float32 and float64 copies of the scaled model
+        return b;
+    }
+    static int sm_count() {
+        int dev = 0, sms = 148;
+        VK_CUDA(cudaGetDevice(&dev));
+        VK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        return sms;
+    }
+    bool over_time(std::chrono::steady_clock::time_point t0) const {
+        return std::isfinite(o_.time_limit_seconds) && seconds_since(t0) >= o_.time_limit_seconds;
+    }
+
+    template <class T>
+    void alloc_state(SState<T> &st, int nov) {
+        const size_t nx = static_cast<size_t>(n_) * ld_, ny = std::max<size_t>(1, static_cast<size_t>(m_) * ld_);
+        const size_t no = std::max<size_t>(1, static_cast<size_t>(nov) * ld_);
+        for (DevBuf<T> *b : {&st.x, &st.x0, &st.xbar, &st.xhat}) b->reset(nx);
+        for (DevBuf<T> *b : {&st.y, &st.y0, &st.yhat}) b->reset(ny);
+        st.ovl.reset(no);
+        st.ovu.reset(no);
+    }
+
+    // Shared scaled model vectors in T (c, bounds, row bounds, scales).
+    template <class T>
+    void state_model(SState<T> &st) {
+        const int n = n_, m = std::max(m_, 1);
+        for (DevBuf<T> *b : {&st.l, &st.u, &st.c, &st.cs}) b->reset(n);
+        for (DevBuf<T> *b : {&st.rl, &st.ru, &st.rs}) b->reset(m);
+        auto &src = base_.s64_;
+        sconvert_kernel<T, double><<<grid1d(n), 256, 0, s_>>>(src.l.get(), n, st.l.get());
+        sconvert_kernel<T, double><<<grid1d(n), 256, 0, s_>>>(src.u.get(), n, st.u.get());
+        sconvert_kernel<T, double><<<grid1d(n), 256, 0, s_>>>(src.c.get(), n, st.c.get());
+        sconvert_kernel<T, double><<<grid1d(n), 256, 0, s_>>>(base_.cs_.get(), n, st.cs.get());
+        if (m_ > 0) {
+            sconvert_kernel<T, double><<<grid1d(m_), 256, 0, s_>>>(src.rl.get(), m_, st.rl.get());
+            sconvert_kernel<T, double><<<grid1d(m_), 256, 0, s_>>>(src.ru.get(), m_, st.ru.get());
+            sconvert_kernel<T, double><<<grid1d(m_), 256, 0, s_>>>(base_.rs_.get(), m_, st.rs.get());
+        }
+        VK_LAUNCH_CHECK();
+    }
+
+    template <class TD, class TS>
+    void copy_state(const SState<TS> &a, SState<TD> &b, int nov, bool bounds) {
+        const int64_t nx = static_cast<int64_t>(n_) * ld_, ny = static_cast<int64_t>(m_) * ld_;
+        for (auto pr : {std::make_pair(&a.x, &b.x), std::make_pair(&a.x0, &b.x0), std::make_pair(&a.xhat, &b.xhat),
+                        std::make_pair(&a.xbar, &b.xbar)})
+            sconvert_kernel<TD, TS><<<grid_for64(nx), 256, 0, s_>>>(pr.first->get(), nx, pr.second->get());
+        if (ny > 0)
+            for (auto pr : {std::make_pair(&a.y, &b.y), std::make_pair(&a.y0, &b.y0), std::make_pair(&a.yhat, &b.yhat)})
+                sconvert_kernel<TD, TS><<<grid_for64(ny), 256, 0, s_>>>(pr.first->get(), ny, pr.second->get());
+        if (bounds && nov > 0) {
+            const int64_t no = static_cast<int64_t>(nov) * ld_;
+            sconvert_kernel<TD, TS><<<grid_for64(no), 256, 0, s_>>>(a.ovl.get(), no, b.ovl.get());
+            sconvert_kernel<TD, TS><<<grid_for64(no), 256, 0, s_>>>(a.ovu.get(), no, b.ovu.get());
+        }
+        VK_LAUNCH_CHECK();
+    }
+
+    void control_arrays() {
+        const size_t Bs = B_;
+        for (DevBuf<double> *d : {&eta_, &omega_, &tau_, &sigma_, &rr_, &rp_, &bn_, &cn_, &off_, &kkt_, &relp_, &reld_,
+                                  &relg_})
+            d->reset(Bs);
+        for (DevBuf<long long> *d : {&kb_, &it_, &rst_}) d->reset(Bs);
+        for (DevBuf<int> *d : {&done_, &status_, &rnow_}) d->reset(Bs);
+        h_done_.resize(B_);
+        h_status_.resize(B_);
+        h_iters_.resize(B_);
+        h_restarts_.resize(B_);
+        h_kkt_.resize(B_);
+        h_rel_p_.resize(B_);
+        h_rel_d_.resize(B_);
+        h_rel_gap_.resize(B_);
+    }
+
+    BCtl ctl() {
+        BCtl c{};
+        c.eta = eta_.get();
+        c.omega = omega_.get();
+        c.tau = tau_.get();
+        c.sigma = sigma_.get();
+        c.r_restart = rr_.get();
+        c.r_prev = rp_.get();
+        c.bnorm = bn_.get();
+        c.cnorm = cn_.get();
+        c.offset = off_.get();
+        c.kkt = kkt_.get();
+        c.rel_p = relp_.get();
+        c.rel_d = reld_.get();
+        c.rel_gap = relg_.get();
+        c.k_base = kb_.get();
+        c.iters = it_.get();
+        c.restarts = rst_.get();
+        c.done = done_.get();
+        c.status = status_.get();
+        c.restart_now = rnow_.get();
+        c.tol = o_.relative_tolerance;
+        c.limit = o_.iteration_limit;
+        c.count = B_;
+        return c;
+    }
+
+    void fill(DevBuf<double> &d, double v) {
+        std::vector<double> h(B_, v);
+        VK_CUDA(cudaMemcpyAsync(d.get(), h.data(), B_ * sizeof(double), cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaStreamSynchronize(s_));
+    }
+
+    void reset_control(const std::vector<int> &invalid) {
+        const double eta = base_.h_eta_[0], w0 = base_.h_omega0_[0];
+        fill(eta_, eta);
+        fill(omega_, w0);
+        fill(tau_, eta / w0);
+        fill(sigma_, eta * w0);
+        fill(rr_, -1.0);
+        fill(rp_, std::numeric_limits<double>::infinity());
+        fill(kkt_, std::numeric_limits<double>::infinity());
+        fill(bn_, base_.bnorm_[0]);
+        fill(cn_, base_.cnorm_[0]);
+        fill(off_, model_.objective_offset);
+        for (DevBuf<long long> *d : {&kb_, &it_, &rst_}) VK_CUDA(cudaMemsetAsync(d->get(), 0, d->bytes(), s_));
+        VK_CUDA(cudaMemsetAsync(rnow_.get(), 0, rnow_.bytes(), s_));
+        std::vector<int> st(B_);
+        for (int b = 0; b < B_; ++b) st[b] = invalid[b] ? VK_STATUS_INVALID_MODEL : VK_STATUS_NOT_SOLVED;
+        VK_CUDA(cudaMemcpyAsync(done_.get(), invalid.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaMemcpyAsync(status_.get(), st.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaStreamSynchronize(s_));
+    }
+
+    void reopen(const std::vector<int> &invalid) {
+        read_control();
+        std::vector<int> done(B_), status(B_);
+        for (int b = 0; b < B_; ++b) {
+            const bool keep = invalid[b] || h_status_[b] == VK_STATUS_NUMERICAL_FAILURE;
+            done[b] = keep ? 1 : 0;
+            status[b] = keep ? h_status_[b] : VK_STATUS_NOT_SOLVED;
+        }
+        VK_CUDA(cudaMemcpyAsync(done_.get(), done.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaMemcpyAsync(status_.get(), status.data(), B_ * sizeof(int), cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaStreamSynchronize(s_));
+    }
+
+    void read_control() {
+        VK_CUDA(cudaMemcpyAsync(h_done_.data(), done_.get(), B_ * sizeof(int), cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaMemcpyAsync(h_status_.data(), status_.get(), B_ * sizeof(int), cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaMemcpyAsync(h_iters_.data(), it_.get(), B_ * sizeof(long long), cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaMemcpyAsync(h_restarts_.data(), rst_.get(), B_ * sizeof(long long), cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaMemcpyAsync(h_kkt_.data(), kkt_.get(), B_ * 8, cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaMemcpyAsync(h_rel_p_.data(), relp_.get(), B_ * 8, cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaMemcpyAsync(h_rel_d_.data(), reld_.get(), B_ * 8, cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaMemcpyAsync(h_rel_gap_.data(), relg_.get(), B_ * 8, cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaStreamSynchronize(s_));
+    }
+
+    template <class T>
+    SpmmMat<T> mat(bool transposed) {
+        const CsrPattern32 &p = transposed ? base_.at_ : base_.a_;
+        const T *val;
+        if constexpr (std::is_same<T, double>::value)
+            val = transposed ? base_.s64_.kat.get() : base_.s64_.ka.get();
+        else
+            val = transposed ? base_.s32_.kat.get() : base_.s32_.ka.get();
+        return SpmmMat<T>{p.ro.get(), p.ci.get(), val, p.rows};
+    }
+
+    template <class T, int VEC, class Epi>
+    void pass(bool transposed, const T *X, const Epi &e) {
+        const int G = ld_ / (32 * VEC);
+        const int P = std::is_same<T, double>::value ? P64_ : P32_;
+        const SpmmMat<T> M = mat<T>(transposed);
+        if (M.rows == 0) return;
+        spmm_kernel<T, VEC, Epi><<<G * P, kSpmmWarps * 32, 0, s_>>>(M, X, ld_, G, e, partial_.get());
+        VK_LAUNCH_CHECK();
+    }
+
+    void reduce(int R, DevBuf<double> &out, int P) {
+        spmm_reduce_kernel<<<grid1d(int64_t(B_) * R), 256, 0, s_>>>(partial_.get(), P, R, ld_, B_, out.get());
+        VK_LAUNCH_CHECK();
+    }
+
+    template <class T, int VEC>
+    cudaGraphExec_t capture(SState<T> &st) {
+        const int P = std::is_same<T, double>::value ? P64_ : P32_;
+        VK_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+        const BCtl c = ctl();
+        // without rows the transposed matrix has n empty rows: the column
+        // passes still run (s = 0) and never read the gathered vector
+        const T *yg = m_ > 0 ? st.y.get() : st.x.get();
+        const T *yhg = m_ > 0 ? st.yhat.get() : st.x.get();
+        for (int it = 0; it < chunk_; ++it) {
+            const bool check = it == chunk_ - 1;
+            if (check) {
+                pass<T, VEC>(true, yg, SColEpi<T, VEC, true>{c, it, ld_, st.x.get(), st.xbar.get(), st.xhat.get(),
+                                                             st.x0.get(), st.c.get(), st.l.get(), st.u.get(),
+                                                             st.ovl.get(), st.ovu.get(), ov_});
+                reduce(2, sc_, P);
+                if (m_ > 0) {
+                    pass<T, VEC>(false, st.xbar.get(),
+                                 SRowEpi<T, VEC, true>{c, it, ld_, st.y.get(), st.yhat.get(), st.y0.get(),
+                                                       st.rl.get(), st.ru.get()});
+                    reduce(2, sr_, P);
+                    pass<T, VEC>(false, st.xhat.get(),
+                                 SKktRowEpi<T, VEC>{c, ld_, st.yhat.get(), st.rl.get(), st.ru.get(), st.rs.get()});
+                    reduce(3, skr_, P);
+                } else {
+                    VK_CUDA(cudaMemsetAsync(sr_.get(), 0, sr_.bytes(), s_));
+                    VK_CUDA(cudaMemsetAsync(skr_.get(), 0, skr_.bytes(), s_));
+                }
+                pass<T, VEC>(true, yhg, SKktColEpi<T, VEC>{c, ld_, st.xhat.get(), st.c.get(), st.l.get(), st.u.get(),
+                                                          st.ovl.get(), st.ovu.get(), st.cs.get(), ov_});
+                reduce(4, skc_, P);
+                batch_control_kernel<<<ceil_div(B_, 128), 128, 0, s_>>>(c, sc_.get(), sr_.get(), skr_.get(),
+                                                                        skc_.get(), chunk_);
+                const int64_t nx = static_cast<int64_t>(n_) * ld_, ny = static_cast<int64_t>(m_) * ld_;
+                srestart_kernel<T><<<grid_for64(std::max(nx, ny)), 256, 0, s_>>>(
+                    c, ld_, st.x.get(), st.x0.get(), st.xhat.get(), nx, st.y.get(), st.y0.get(), st.yhat.get(), ny);
+                VK_LAUNCH_CHECK();
+            } else {
+                pass<T, VEC>(true, yg, SColEpi<T, VEC, false>{c, it, ld_, st.x.get(), st.xbar.get(), st.xhat.get(),
+                                                              st.x0.get(), st.c.get(), st.l.get(), st.u.get(),
+                                                              st.ovl.get(), st.ovu.get(), ov_});
+                if (m_ > 0)
+                    pass<T, VEC>(false, st.xbar.get(),
+                                 SRowEpi<T, VEC, false>{c, it, ld_, st.y.get(), st.yhat.get(), st.y0.get(),
+                                                        st.rl.get(), st.ru.get()});
+            }
+        }
+        cudaGraph_t g;
+        VK_CUDA(cudaStreamEndCapture(s_, &g));
+        size_t nodes = 0;
+        VK_CUDA(cudaGraphGetNodes(g, nullptr, &nodes));
+        nodes_ = static_cast<long long>(nodes);
+        cudaGraphExec_t ex;
+        VK_CUDA(cudaGraphInstantiate(&ex, g, 0));
+        cudaGraphDestroy(g);
+        return ex;
+    }
+
+    vk_options o_;
+    int B_;
+    BatchEngine base_;
+    const vk_problem &model_;
+    int m_ = 0, n_ = 0, ld_ = 0, vec32_ = 1, vec64_ = 1, P32_ = 1, P64_ = 1, pmax_ = 1, chunk_ = 64;
+    bool mixed_ = false;
+    cudaStream_t s_ = nullptr;
+    const int *ov_ = nullptr;
+    SState<double> s64_;
+    SState<float> s32_;
+    DevBuf<double> partial_, sc_, sr_, skr_, skc_;
+    DevBuf<double> eta_, omega_, tau_, sigma_, rr_, rp_, bn_, cn_, off_, kkt_, relp_, reld_, relg_;
+    DevBuf<long long> kb_, it_, rst_;
+    DevBuf<int> done_, status_, rnow_;
+    std::vector<int> h_done_, h_status_;
+    std::vector<long long> h_iters_, h_restarts_;
+    std::vector<double> h_kkt_, h_rel_p_, h_rel_d_, h_rel_gap_;
+    cudaGraphExec_t g64_ = nullptr, g32_ = nullptr;
+    long long nodes_ = 0;
+};
+
 } // namespace
 
 // Validates every instance (LP only) and runs the batch.
@@ -1025,6 +1947,28 @@ void batch_solve(const vk_problem *probs, int count, const vk_options &o, vk_res
         throw Unsupported("the batch exceeds the int32 index range of the device structures");
     BatchEngine eng(probs, count, o);
     eng.solve(results);
+}
+
+
+// Validates the model (LP only) and solves `count` relaxations of it that
+// differ in variable bounds / warm start.
+void batch_solve_shared(const vk_problem &p, int count, const double *lower, const double *upper,
+                        const double *warm, const vk_options &o, vk_result *results) {
+    if (count <= 0) throw InvalidInput("count must be positive");
+    if (o.algorithm != VK_ALGO_HALPERN) throw Unsupported("batched solves use VK_ALGO_HALPERN");
+    bool unsupported = false;
+    const std::string msg = validate_problem(p, o, unsupported);
+    if (!msg.empty()) {
+        if (unsupported) throw Unsupported(msg);
+        throw InvalidInput(msg);
+    }
+    if (p.Q.rows > 0 && p.Q.row_offsets && p.Q.row_offsets[p.Q.rows] > 0)
+        throw Unsupported("batched solves take LPs");
+    const int64_t ld = (static_cast<int64_t>(count) + 127) / 128 * 128;
+    if ((p.A.cols + 1) * ld >= (int64_t(1) << 40) || count >= (1 << 24))
+        throw Unsupported("the batch is too large for one device");
+    SharedEngine eng(p, count, o);
+    eng.solve(lower, upper, warm, results);
 }
 
 } // namespace vk

@@ -375,4 +375,20 @@ int vk_batch_solve(const vk_problem *problems, int32_t count, const vk_options *
     });
 }
 
+int vk_batch_solve_shared(const vk_problem *problem, int32_t count, const double *lower, const double *upper,
+                          const double *warm, const vk_options *opts, vk_result *results) {
+    return guarded([&] {
+        if (!problem || !results || count <= 0) return set_error(VK_ERR_INVALID, "invalid argument");
+        vk_options o;
+        if (opts)
+            o = *opts;
+        else {
+            vk_default_options(&o);
+            o.algorithm = VK_ALGO_HALPERN;
+        }
+        vk::batch_solve_shared(*problem, count, lower, upper, warm, o, results);
+        return VK_OK;
+    });
+}
+
 } // extern "C"

@@ -71,5 +71,8 @@ std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s);
 
 // Independent LPs solved together (vk_batch.cu); throws on invalid input.
 void batch_solve(const vk_problem *problems, int count, const vk_options &o, vk_result *results);
+// Relaxations of one LP differing in variable bounds / warm start (vk_batch.cu).
+void batch_solve_shared(const vk_problem &p, int count, const double *lower, const double *upper,
+                        const double *warm, const vk_options &o, vk_result *results);
 
 } // namespace vk
