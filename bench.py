@@ -18,6 +18,9 @@ replicas, no collective on the path). The same line carries:
   time_to_tol    time and iterations to 1e-6 relative KKT (small LP and, with
                  --ttt, the large LP), fp64 vs mixed
   spmv           GB/s of the sparse product kernel, A x and A'y, fp64 / fp32
+  batched        768 LPs (512 shared-matrix node relaxations + 256 independent
+                 LPs) to 1e-6 relative KKT in two batches, mixed and fp64, vs
+                 the plain fp64 engine one instance at a time (sampled)
   roofline       the sparse-pass kernel against measured HBM bandwidth
   cpu_baseline   the reference's CPU implementation on this host
 `python bench.py --impl reference` times the reference's own CPU PDHG
@@ -187,6 +190,76 @@ def time_to_tolerance(inst, label, limit, time_limit=float("inf")):
     return res
 
 
+def batched_figures(sample_every=64):
+    """The batched workload: 512 node relaxations of one LP (m=50,000, n=100,000,
+    6 nonzeros per column, 1-12 tightened variables each) and 256 independent
+    LPs (m log-uniform on [500, 20000], n=2m, 8 per column), all to 1e-6
+    relative KKT. Both batches run at once (two host threads, two streams);
+    wall time from host arrays to results. The plain-FP64 comparison solves
+    instances one by one with the single-instance float64 engine (a resident
+    model for the nodes, create+solve for each independent LP) on a systematic
+    sample (every `sample_every`-th node, every (sample_every/2)-th LP) and
+    scales the sample's mean to the whole set."""
+    import vikalp_b200 as vk
+    from vikalp_b200 import synthetic
+    node_lp = synthetic.lp_uniform(50000, 100000, 6, seed=2025)
+    lo, hi = synthetic.bnb_nodes(node_lp, 512, seed=7)
+    indep = synthetic.workload_independent_lps(256)
+    tol = dict(iteration_limit=200000, relative_tolerance=1e-6, time_limit_seconds=300)
+
+    def run(prec):
+        res = {}
+
+        def shared():
+            t = time.perf_counter()
+            res["shared"] = vk.batch_solve_shared(node_lp, 512, lo, hi, precision=prec, **tol)
+            res["shared_s"] = time.perf_counter() - t
+
+        def independent():
+            t = time.perf_counter()
+            res["indep"] = vk.batch_solve(indep, precision=prec, **tol)
+            res["indep_s"] = time.perf_counter() - t
+
+        t0 = time.perf_counter()
+        th = [threading.Thread(target=shared), threading.Thread(target=independent)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        wall = time.perf_counter() - t0
+        rs = res["shared"] + res["indep"]
+        status = {}
+        for r in rs:
+            status[r["status"]] = status.get(r["status"], 0) + 1
+        return {"wall_s": round(wall, 3), "shared_s": round(res["shared_s"], 3), "independent_s": round(res["indep_s"], 3),
+                "shared_iterate_s": round(res["shared"][0]["iterate_seconds"], 3),
+                "independent_iterate_s": round(res["indep"][0]["iterate_seconds"], 3),
+                "status": status, "max_iterations": int(max(r["iterations"] for r in rs)),
+                "max_rel_kkt": float(max(max(r["rel_primal"], r["rel_dual"], r["rel_gap"]) for r in rs))}
+
+    out = {"workload": "512 node LPs sharing A (m=5e4 n=1e5 nnz=600k, 1-12 tightened bounds) + 256 independent LPs "
+                       "(m log-uniform 500..20000, n=2m, 8/col; 19.7M nnz), to 1e-6 relative KKT",
+           "mixed": run("mixed"), "fp64_batched": run("fp64")}
+    # plain float64, one instance at a time (sample)
+    node_t, indep_t = [], []
+    with vk.Pdhg(node_lp, algorithm="halpern", precision="fp64", **tol) as h:
+        for b in range(0, 512, sample_every):
+            t = time.perf_counter()
+            r = h.solve(lower=lo[b], upper=hi[b], duals=False)
+            node_t.append(time.perf_counter() - t)
+            assert r["status"] == "Optimal", r["status"]
+    for b in range(0, 256, sample_every // 2):
+        t = time.perf_counter()
+        r = vk.solve(indep[b], algorithm="halpern", precision="fp64", **tol)
+        indep_t.append(time.perf_counter() - t)
+    est = 512 * statistics.mean(node_t) + 256 * statistics.mean(indep_t)
+    out["plain_fp64_one_by_one"] = {"estimated_s": round(est, 3), "node_sample_s": [round(t, 4) for t in node_t],
+                                    "independent_sample_s": [round(t, 4) for t in indep_t],
+                                    "sample": f"{len(node_t)} of 512 nodes, {len(indep_t)} of 256 LPs, mean x count"}
+    out["speedup_mixed_batched_vs_plain_fp64"] = round(est / out["mixed"]["wall_s"], 2)
+    return out
+
+
 def reference_cpu_rate(inst, budget_s):
     """Iterations/s of the reference's own CPU PDHG iteration (pdhg.cpp:92-130 call
     sequence through its CPU ExecutionBackend), a bounded sample sized by budget_s."""
@@ -209,6 +282,7 @@ def main():
     ap.add_argument("--ttt", action="store_true", help="also time the large LP to 1e-6 relative KKT")
     ap.add_argument("--ttt-seconds", type=float, default=60.0, help="time cap per precision for --ttt")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-workload figures")
     ap.add_argument("--profile-spmv", choices=["fp64", "fp32"], default=None,
                     help="only run the sparse-product kernel 5 times on the large LP (for ncu captures)")
     ap.add_argument("--transpose", action="store_true", help="with --profile-spmv: A'y instead of A x")
@@ -306,6 +380,8 @@ def main():
         if args.ttt:
             ttt["large_lp"] = time_to_tolerance(inst, "large lp", 2_000_000, time_limit=args.ttt_seconds)
         line["time_to_tol"] = ttt
+        if not args.no_batched:
+            line["batched"] = batched_figures()
         if ws == 1:
             rate, n_it, secs = reference_cpu_rate(inst, budget_s=20.0)
             line["cpu_baseline"] = {"value": round(rate, 4), "unit": "iter/s", "cores": 1, "kind": "reference",

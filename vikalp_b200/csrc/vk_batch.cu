@@ -392,8 +392,12 @@ public:
         VK_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
         mixed_ = o.precision == VK_PREC_MIXED;
         chunk_ = std::max(2, o.check_every > 0 ? o.check_every : 64);
+        log_.stream(s_);
+        log_.mark("stream");
         concatenate(probs);
+        log_.mark("concatenate (host)");
         setup_device();
+        log_.mark("step sizes");
     }
     ~BatchEngine() {
         if (g64_) cudaGraphExecDestroy(g64_);
@@ -595,8 +599,10 @@ private:
         build_tiles(at_, s_, dcb.get());
         DevBuf<double> at_val(padded(nnz_));
         gather_values<double, double>(perm_.get(), a_val.get(), at_val.get(), nnz_, s_);
+        log_.mark("upload + transpose");
         autotune_pattern<double>(a_, a_val.get(), s_);
         autotune_pattern<double>(at_, at_val.get(), s_);
+        log_.mark("autotune");
         up(rinst_, h_rinst_);
         up(cinst_, h_cinst_);
         // instance of each tile and each instance's first tile
@@ -631,8 +637,10 @@ private:
                 VK_LAUNCH_CHECK();
             }
         }
+        log_.mark("scaling");
         setup_state(s64_, a_val, at_val, c, rl, ru);
         if (mixed_) setup_state(s32_, a_val, at_val, c, rl, ru);
+        log_.mark("scaled copies");
         // model bounds, scaled, into the float64 state (the float32 copy is made per solve)
         bscale_vec_kernel<double><<<grid1d(n_), 256, 0, s_>>>(vl.get(), cs_.get(), n_, 1, s64_.l.get());
         bscale_vec_kernel<double><<<grid1d(n_), 256, 0, s_>>>(vu.get(), cs_.get(), n_, 1, s64_.u.get());
@@ -963,6 +971,7 @@ private:
 
     vk_options o_;
     int B_;
+    PhaseLog log_{o_.verbose, "batch", nullptr};
     cudaStream_t s_ = nullptr;
     bool mixed_ = false;
     int chunk_ = 64;
@@ -1465,6 +1474,7 @@ public:
 
     void solve(const double *lower, const double *upper, const double *warm, vk_result *results) {
         const auto started = std::chrono::steady_clock::now();
+        PhaseLog lg(o_.verbose, "shared", s_);
         const int n = n_, m = m_;
         // per-instance checks (continuous_common.hpp:80-110, pdhg.cpp:29-33)
         std::vector<int> invalid(B_, 0);
@@ -1495,6 +1505,7 @@ public:
                 ov_cols.push_back(j);
             }
         const int nov = static_cast<int>(ov_cols.size());
+        lg.mark("instance checks (host)");
         // bounds and warm start of every instance, on the device
         const size_t bn = static_cast<size_t>(B_) * n;
         DevBuf<double> dlo(bn), dhi(bn), dwarm(warm ? bn : 1);
@@ -1540,6 +1551,7 @@ public:
         VK_CUDA(cudaMemsetAsync(s64_.xbar.get(), 0, nx * sizeof(double), s_));
         ov_ = dov_index.get();
         reset_control(invalid);
+        lg.mark("upload + start points");
 
         cudaEvent_t e0, e1;
         VK_CUDA(cudaEventCreate(&e0));
@@ -1560,6 +1572,7 @@ public:
             state_model(s32_);
             copy_state<float, double>(s64_, s32_, nov, true);
             g32_ = vec32_ == 4 ? capture<float, 4>(s32_) : capture<float, 1>(s32_);
+            lg.mark("float32 state + graph");
             std::vector<double> best(B_, std::numeric_limits<double>::infinity());
             int stall = 0;
             for (;;) {
@@ -1589,6 +1602,7 @@ public:
                     break;
             }
             fp32_iters = h_iters_.empty() ? 0 : *std::max_element(h_iters_.begin(), h_iters_.end());
+            lg.mark("float32 iterations");
             copy_state<double, float>(s32_, s64_, nov, false);
             reopen(invalid);
         }
@@ -1606,6 +1620,7 @@ public:
                 if (std::all_of(h_done_.begin(), h_done_.end(), [](int d) { return d != 0; })) break;
             }
         }
+        lg.mark("float64 iterations");
         VK_CUDA(cudaEventRecord(e1, s_));
         read_control();
         float ms = 0.f;
@@ -1625,6 +1640,7 @@ public:
         if (m > 0)
             VK_CUDA(cudaMemcpyAsync(hy.data(), yo.get(), hy.size() * sizeof(double), cudaMemcpyDeviceToHost, s_));
         VK_CUDA(cudaStreamSynchronize(s_));
+        lg.mark("results to host");
         const double secs = seconds_since(started);
         for (int b = 0; b < B_; ++b) {
             vk_result &r = results[b];

@@ -42,4 +42,26 @@ inline double seconds_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// Host-side phase timings on stderr when vk_options::verbose > 0
+// (`stream` is synchronized first so device work is attributed to its phase).
+class PhaseLog {
+public:
+    PhaseLog(int verbose, const char *who, cudaStream_t s) : on_(verbose > 0), who_(who), s_(s) {}
+    void mark(const char *what) {
+        if (!on_) return;
+        cudaStreamSynchronize(s_);
+        const auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "[vikalp_b200] %s: %-28s %8.3f s\n", who_, what,
+                     std::chrono::duration<double>(now - t_).count());
+        t_ = now;
+    }
+    void stream(cudaStream_t s) { s_ = s; }
+
+private:
+    bool on_;
+    const char *who_;
+    cudaStream_t s_;
+    std::chrono::steady_clock::time_point t_ = std::chrono::steady_clock::now();
+};
+
 } // namespace vk
