@@ -65,36 +65,89 @@ def sigma_max(K: sp.csr_matrix, iters: int = 200) -> float:
     return prev
 
 
+def _q(inst):
+    """Q as a scipy CSR matrix, or None for an LP."""
+    if getattr(inst, "q_col_idx", None) is None or inst.q_nnz == 0:
+        return None
+    return sp.csr_matrix((inst.q_values, inst.q_col_idx, inst.q_row_offsets), shape=(inst.n, inst.n))
+
+
+def lambda_max(Q: sp.csr_matrix, iters: int = 200) -> float:
+    """Largest eigenvalue of a PSD matrix by power iteration (same start vector
+    and stopping rule as sigma_max)."""
+    n = Q.shape[0]
+    i = np.arange(n, dtype=np.uint64)
+    h = (i * np.uint64(2654435761) + np.uint64(12345)) & np.uint64(0xFFFFFFFF)
+    h ^= h >> np.uint64(13)
+    h = (h * np.uint64(2246822519)) & np.uint64(0xFFFFFFFF)
+    h ^= h >> np.uint64(16)
+    v = 0.5 + (h & np.uint64(0xFFFF)).astype(np.float64) / 65536.0
+    v /= np.linalg.norm(v)
+    prev = 0.0
+    for it in range(iters):
+        z = Q @ v
+        est = np.linalg.norm(z)
+        v = z / est if est > 0 else z
+        if it > 10 and abs(est - prev) <= 1e-6 * est:
+            return est
+        prev = est
+    return prev
+
+
+def step_params(knorm: float, lq: float, omega: float):
+    """(eta, rho) for primal weight omega: tau = eta/omega, sigma = eta*omega.
+
+    LP (lq == 0): eta = 0.99/|K|, rho = 1 (fully reflected). QP: the explicit
+    gradient step on 0.5 x'Qx needs 1/tau - sigma |K|^2 >= L (L = lambda_max of
+    the scaled Q); eta solves tau L + eta^2 |K|^2 = 0.99^2, and the reflection
+    is cut to rho = 0.99 (1 - 1/(2 kappa)), kappa = (1/tau - sigma |K|^2) / L,
+    which keeps (1+rho) T - rho I nonexpansive (Condat's relaxation bound)."""
+    if lq <= 0:
+        return (0.99 / knorm if knorm > 0 else 1.0), 1.0
+    k2, b, c = knorm * knorm, lq / omega, 0.9801
+    eta = 2.0 * c / (b + np.sqrt(b * b + 4.0 * k2 * c))
+    tau = eta / omega
+    kappa = (1.0 - eta * eta * k2) / (tau * lq)
+    return eta, min(1.0, 0.99 * (1.0 - 1.0 / (2.0 * kappa)))
+
+
 def rel_kkt(inst, x, y, lower=None, upper=None):
     """Relative KKT of (x, y) in original units (same definition as the C oracle)."""
     A = _csr(inst)
+    Q = _q(inst)
     lo = inst.var_lower if lower is None else lower
     hi = inst.var_upper if upper is None else upper
     ax = A @ x
     rl, ru = inst.row_lower, inst.row_upper
     rp = np.linalg.norm(ax - np.clip(ax, rl, ru)) + np.linalg.norm(x - np.clip(x, lo, hi))
     b = np.maximum(np.where(np.isfinite(rl), np.abs(rl), 0), np.where(np.isfinite(ru), np.abs(ru), 0))
-    lam = inst.c + A.T @ y
+    qx = Q @ x if Q is not None else np.zeros_like(x)
+    quad = float(x @ qx)
+    lam = inst.c + qx + A.T @ y
     yl, yu = np.maximum(0, -y), np.maximum(0, y)
     vl, vu = np.maximum(0, lam), np.maximum(0, -lam)
     viol = np.sum(np.where((yl > 0) & ~np.isfinite(rl), yl, 0) ** 2) + np.sum(np.where((yu > 0) & ~np.isfinite(ru), yu, 0) ** 2)
     rd2 = np.sum(np.where((vl > 0) & ~np.isfinite(lo), vl, 0) ** 2) + np.sum(np.where((vu > 0) & ~np.isfinite(hi), vu, 0) ** 2)
     fin = lambda v, w: np.where((w > 0) & np.isfinite(v), np.where(np.isfinite(v), v, 0.0) * w, 0.0)  # noqa: E731
-    dobj = np.sum(fin(rl, yl)) - np.sum(fin(ru, yu)) + np.sum(fin(lo, vl)) - np.sum(fin(hi, vu))
-    pobj = inst.c @ x
+    off = float(getattr(inst, "objective_offset", 0.0))
+    dobj = np.sum(fin(rl, yl)) - np.sum(fin(ru, yu)) + np.sum(fin(lo, vl)) - np.sum(fin(hi, vu)) - 0.5 * quad + off
+    pobj = inst.c @ x + 0.5 * quad + off
     return dict(rel_primal=rp / (1 + np.linalg.norm(b)), rel_dual=np.sqrt(rd2 + viol) / (1 + np.linalg.norm(inst.c)),
                 rel_gap=abs(pobj - dobj) / (1 + abs(pobj) + abs(dobj)), primal_objective=pobj, dual_objective=dobj)
 
 
-def solve(inst, tol=1e-6, iteration_limit=100000, check_every=64, rho=1.0, warm=None, lower=None, upper=None,
+def solve(inst, tol=1e-6, iteration_limit=100000, check_every=64, rho=None, warm=None, lower=None, upper=None,
           trace=False, theta=0.5, omega0=None):
+    """rho: reflection override (default: step_params' choice, 1 for an LP)."""
     A = _csr(inst)
+    Q = _q(inst)
     m, n = A.shape
     lo0 = inst.var_lower if lower is None else lower
     hi0 = inst.var_upper if upper is None else upper
     r, d = scaling(A)
     K = (sp.diags(r) @ A @ sp.diags(d)).tocsr()
     KT = K.T.tocsr()
+    Qs = (sp.diags(d) @ Q @ sp.diags(d)).tocsr() if Q is not None else None
     c = inst.c * d
     with np.errstate(invalid="ignore", divide="ignore"):
         lo = np.where(np.isfinite(lo0), lo0 / d, lo0)
@@ -109,7 +162,9 @@ def solve(inst, tol=1e-6, iteration_limit=100000, check_every=64, rho=1.0, warm=
     if omega0 is not None:
         omega = omega0
     smax = sigma_max(K) if K.nnz else 0.0
-    eta = 0.99 / smax if smax > 0 else 1.0
+    lq = lambda_max(Qs) if Qs is not None and Qs.nnz else 0.0
+    eta, rho_k = step_params(smax, lq, omega)
+    rho_k = rho_k if rho is None else rho
     tau, sigma = eta / omega, eta * omega
     x = np.clip(np.zeros(n) if warm is None else warm / d, lo, hi)
     y = np.zeros(m)
@@ -121,12 +176,13 @@ def solve(inst, tol=1e-6, iteration_limit=100000, check_every=64, rho=1.0, warm=
     while True:
         for it in range(check_every):
             lam = (k_base + it + 1.0) / (k_base + it + 2.0)
-            xh = np.clip(x - tau * (c + KT @ y), lo, hi)
+            g = c + KT @ y if Qs is None else c + Qs @ x + KT @ y
+            xh = np.clip(x - tau * g, lo, hi)
             xb = 2 * xh - x
-            xn = lam * ((1 + rho) * xh - rho * x) + (1 - lam) * x0
+            xn = lam * ((1 + rho_k) * xh - rho_k * x) + (1 - lam) * x0
             v = y + sigma * (K @ xb)
             yh = v - np.clip(v, sigma * rl, sigma * ru)
-            yn = lam * ((1 + rho) * yh - rho * y) + (1 - lam) * y0
+            yn = lam * ((1 + rho_k) * yh - rho_k * y) + (1 - lam) * y0
             if it == check_every - 1:
                 dx2, dx0 = np.sum((xh - x) ** 2), np.sum((xh - x0) ** 2)
                 dy2, dy0 = np.sum((yh - y) ** 2), np.sum((yh - y0) ** 2)
@@ -153,6 +209,8 @@ def solve(inst, tol=1e-6, iteration_limit=100000, check_every=64, rho=1.0, warm=
             mx, my = np.sqrt(dx0), np.sqrt(dy0)
             if mx > 1e-10 and my > 1e-10:
                 omega = np.exp(theta * np.log(my / mx) + (1 - theta) * np.log(omega))
+            eta, rho_k = step_params(smax, lq, omega)
+            rho_k = rho_k if rho is None else rho
             tau, sigma = eta / omega, eta * omega
             k_base = 0
             restarts += 1

@@ -97,8 +97,30 @@ def test_iteration_and_time_limits(lp_mid):
     assert r["status"] == "TimeLimit" and r["solve_seconds"] < 5.0
 
 
-def test_qp_rejected_by_halpern():
-    q = synthetic.qp_sparse(30, 60, 3, b_rows=10, seed=1)
-    with pytest.raises(vk.VkError) as e:
-        vk.Pdhg(q, algorithm="halpern")
-    assert e.value.code == vk.VK_ERR_UNSUPPORTED
+@pytest.fixture(scope="module")
+def qp_small():
+    return synthetic.qp_sparse(300, 800, 5, b_rows=100, seed=1)
+
+
+def test_qp_iterates_match_restatement(qp_small):
+    # PDQP: Q pass + explicit gradient step, step sizes from |K| and
+    # lambda_max(Q^), reflection cut below 1
+    want = halpern.solve(qp_small, tol=0.0, iteration_limit=192, check_every=64)
+    got = vk.solve(qp_small, algorithm="halpern", iteration_limit=192, relative_tolerance=0.0, check_every=64)
+    assert got["iterations"] == want["iterations"] == 192
+    assert got["restarts"] == want["restarts"]
+    for k in ("x", "y"):
+        scale = 1.0 + np.abs(want[k]).max()
+        assert np.max(np.abs(got[k] - want[k])) <= 1e-8 * scale, k
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_qp_solves_to_relative_kkt(qp_small, oracle, precision):
+    r = vk.solve(qp_small, algorithm="halpern", precision=precision, iteration_limit=400000, relative_tolerance=1e-6)
+    assert r["status"] == "Optimal", r["message"]
+    # the C oracle's KKT of the returned point: feasibility + zero gap certify
+    # optimality of a convex QP
+    k = oracle.rel_kkt(qp_small, r["x"], r["y"])
+    assert max(k["rel_primal"], k["rel_dual"], k["rel_gap"]) <= KKT_TOL, k
+    # objective of the restatement run to 1e-8 relative KKT (48.0767314906966)
+    assert abs(r["objective"] - 48.0767314906966) <= 1e-5 * 49.0

@@ -43,22 +43,42 @@
 namespace vk {
 namespace {
 
-constexpr double kRho = 1.0;           // reflection (1 = fully reflected)
 constexpr int kRuizPasses = 10;
 constexpr int kPowerMax = 200;
 constexpr int kColCheckSums = 2;       // |x^-x|^2, |x^-x0|^2
 constexpr int kRowCheckSums = 2;       // |y^-y|^2, |y^-y0|^2
 constexpr int kKktRowSums = 3;         // primal res^2, dual-obj rows, row-dual violations^2
-constexpr int kKktColSums = 4;         // dual res^2, dual-obj cols, primal obj, box violation^2
+constexpr int kKktColSums = 5;         // dual res^2, dual-obj cols, primal obj, box violation^2, x'Qx
 
 struct HalCtl {
     double eta, omega, tau, sigma;
     double r_restart, r_prev;
     double rel_p, rel_d, rel_gap, kkt;
     double bnorm, cnorm, offset, tol;
+    double knorm, lq, rho, pad_d; // sigma_max(K), lambda_max(Q^) (0: LP), reflection
     long long k_base, total, limit, restarts, checks;
     int done, status, restart_now, pad;
 };
+
+// Step sizes for primal weight omega: tau = eta/omega, sigma = eta*omega.
+// LP (lq == 0): eta = 0.99/|K| and full reflection rho = 1. QP: the explicit
+// gradient step on 0.5 x'Q^x needs 1/tau - sigma |K|^2 >= L; eta solves
+// tau L + eta^2 |K|^2 = 0.99^2 and the reflection is cut to
+// rho = 0.99 (1 - 1/(2 kappa)), kappa = (1/tau - sigma |K|^2) / L, which keeps
+// (1+rho) T - rho I nonexpansive (Condat's bound on the relaxation of the
+// primal-dual iteration with a smooth term).
+__host__ __device__ inline void step_params(double knorm, double lq, double omega, double &eta, double &rho) {
+    if (!(lq > 0.0)) {
+        eta = knorm > 0.0 ? 0.99 / knorm : 1.0;
+        rho = 1.0;
+        return;
+    }
+    const double k2 = knorm * knorm, b = lq / omega, c = 0.9801;
+    eta = 2.0 * c / (b + sqrt(b * b + 4.0 * k2 * c));
+    const double tau = eta / omega;
+    const double kappa = (1.0 - eta * eta * k2) / (tau * lq);
+    rho = fmin(1.0, 0.99 * (1.0 - 1.0 / (2.0 * kappa)));
+}
 
 // ---- scaling (FP64, original values) -----------------------------------------
 
@@ -156,26 +176,28 @@ __device__ __forceinline__ double halpern_lambda(const HalCtl *c, int it) {
     return (k + 1.0) / (k + 2.0);
 }
 
+// Columns (gathers y): qx = Q^ x from the preceding Q pass (QP) or null (LP).
 template <class T, bool CHECK>
 struct HalColEpi : EpiBase<T> {
     static constexpr int NR = CHECK ? kColCheckSums : 1;
     const HalCtl *ctl;
     int it;
     T *x, *xbar, *xhat;
-    const T *x0, *c, *l, *u;
+    const T *x0, *c, *l, *u, *qx;
     double *partials;
     struct Pre {
-        T x, x0, c, l, u;
+        T x, x0, c, l, u, q;
     };
     __device__ bool skip() const { return ctl->done != 0; }
-    __device__ Pre load(int j) const { return Pre{x[j], x0[j], c[j], l[j], u[j]}; }
+    __device__ Pre load(int j) const { return Pre{x[j], x0[j], c[j], l[j], u[j], qx ? qx[j] : T(0)}; }
     __device__ void row_pre(int j, const T (&s)[1], const Pre &p, double (&red)[NR]) const {
         const T tau = static_cast<T>(ctl->tau);
+        const T rho = static_cast<T>(ctl->rho);
         const T lam = static_cast<T>(halpern_lambda(ctl, it));
-        const T xh = clampbox(p.x - tau * (p.c + s[0]), p.l, p.u);
+        const T xh = clampbox(p.x - tau * (p.c + p.q + s[0]), p.l, p.u);
         const T xb = T(2) * xh - p.x;
         xbar[j] = xb;
-        x[j] = lam * ((T(1) + T(kRho)) * xh - T(kRho) * p.x) + (T(1) - lam) * p.x0;
+        x[j] = lam * ((T(1) + rho) * xh - rho * p.x) + (T(1) - lam) * p.x0;
         if (CHECK) {
             xhat[j] = xh;
             const double d0 = static_cast<double>(xh) - static_cast<double>(p.x);
@@ -207,10 +229,11 @@ struct HalRowEpi : EpiBase<T> {
     __device__ Pre load(int i) const { return Pre{y[i], y0[i], rl[i], ru[i]}; }
     __device__ void row_pre(int i, const T (&s)[1], const Pre &p, double (&red)[NR]) const {
         const T sigma = static_cast<T>(ctl->sigma);
+        const T rho = static_cast<T>(ctl->rho);
         const T lam = static_cast<T>(halpern_lambda(ctl, it));
         const T v = p.y + sigma * s[0];
         const T yh = v - clampbox(v, sigma * p.rl, sigma * p.ru);
-        y[i] = lam * ((T(1) + T(kRho)) * yh - T(kRho) * p.y) + (T(1) - lam) * p.y0;
+        y[i] = lam * ((T(1) + rho) * yh - rho * p.y) + (T(1) - lam) * p.y0;
         if (CHECK) {
             yhat[i] = yh;
             const double d0 = static_cast<double>(yh) - static_cast<double>(p.y);
@@ -260,20 +283,22 @@ struct KktRowEpi : EpiBase<T> {
     }
 };
 
-// Columns: gathers y^; lambda^ = c^ + K'y^, lambda = lambda^ / D.
+// Columns: gathers y^; lambda^ = c^ + Q^x^ + K'y^, lambda = lambda^ / D
+// (qx = Q^ x^ from a Q pass, null for an LP).
 template <class T>
 struct KktColEpi : EpiBase<T> {
     static constexpr int NR = kKktColSums;
     const HalCtl *ctl;
-    const T *xhat, *c, *l, *u, *cs;
+    const T *xhat, *c, *l, *u, *cs, *qx;
     double *partials;
     struct Pre {
-        T x, c, l, u, d;
+        T x, c, l, u, d, q;
     };
     __device__ bool skip() const { return ctl->done != 0; }
-    __device__ Pre load(int j) const { return Pre{xhat[j], c[j], l[j], u[j], cs[j]}; }
+    __device__ Pre load(int j) const { return Pre{xhat[j], c[j], l[j], u[j], cs[j], qx ? qx[j] : T(0)}; }
     __device__ void row_pre(int, const T (&s)[1], const Pre &p, double (&red)[NR]) const {
-        const double lam = static_cast<double>(p.c) + static_cast<double>(s[0]);
+        const double q = static_cast<double>(p.q);
+        const double lam = static_cast<double>(p.c) + q + static_cast<double>(s[0]);
         const double d = static_cast<double>(p.d);
         const double lo = static_cast<double>(p.l), hi = static_cast<double>(p.u), x = static_cast<double>(p.x);
         const double vl = smax(0.0, lam), vu = smax(0.0, -lam);
@@ -286,12 +311,22 @@ struct KktColEpi : EpiBase<T> {
         red[2] += static_cast<double>(p.c) * x;
         const double bx = (x - clampbox(x, lo, hi)) * d;
         red[3] += bx * bx;
+        red[4] += x * q;
     }
     __device__ void finish(double (&red)[NR], double *scratch, int block) const {
         block_sum<NR>(red, scratch);
         if (threadIdx.x == 0)
             for (int r = 0; r < NR; ++r) partials[(size_t)block * NR + r] = red[r];
     }
+};
+
+// qx = Q^ v, skipped once the solve is done.
+template <class T>
+struct QStore : EpiRow<T, QStore<T>> {
+    const HalCtl *ctl;
+    T *y;
+    __device__ bool skip() const { return ctl->done != 0; }
+    __device__ void row(int i, const T (&s)[1], double (&)[1]) const { y[i] = s[0]; }
 };
 
 template <class T>
@@ -335,8 +370,9 @@ __global__ void __launch_bounds__(kControlThreads)
     HalCtl c = *ctl;
     const double dx2 = s[0], dx0 = s[1], dy2 = s[2], dy0 = s[3];
     const double rp2 = s[4], dobj_r = s[5], viol2 = s[6];
-    const double rd2 = s[7], dobj_c = s[8], pobj = s[9] + c.offset, box2 = s[10];
-    const double dobj = dobj_r + dobj_c + c.offset;
+    const double rd2 = s[7], dobj_c = s[8], box2 = s[10], quad = s[11];
+    const double pobj = s[9] + 0.5 * quad + c.offset;
+    const double dobj = dobj_r + dobj_c - 0.5 * quad + c.offset;
     c.total += chunk;
     c.checks += 1;
     c.rel_p = (sqrt(rp2) + sqrt(box2)) / (1.0 + c.bnorm);
@@ -367,6 +403,7 @@ __global__ void __launch_bounds__(kControlThreads)
         if (restart) {
             const double mx = sqrt(dx0), my = sqrt(dy0);
             if (mx > 1e-10 && my > 1e-10) c.omega = exp(0.5 * log(my / mx) + 0.5 * log(c.omega));
+            step_params(c.knorm, c.lq, c.omega, c.eta, c.rho);
             c.tau = c.eta / c.omega;
             c.sigma = c.eta * c.omega;
             c.k_base = 0;
@@ -426,6 +463,7 @@ struct HalState {
     DevBuf<T> ka, kat;                      // K values, CSR and transposed order
     DevBuf<T> c, l, u, rl, ru, rs, cs;      // scaled data and the scales
     DevBuf<T> x, x0, xbar, xhat, y, y0, yhat;
+    DevBuf<T> q, qx;                        // QP: Q^ = D Q D values, Q^ x
 };
 
 class HalpernEngine final : public Engine {
@@ -442,11 +480,10 @@ public:
         step_size();
         ctl_.reset(1);
         hctl_.reset(1);
-        const size_t pbytes = static_cast<size_t>(kMaxGrid) * 4;
-        pc_.reset(pbytes);
-        pr_.reset(pbytes);
-        pkr_.reset(pbytes);
-        pkc_.reset(pbytes);
+        pc_.reset(static_cast<size_t>(kMaxGrid) * kColCheckSums);
+        pr_.reset(static_cast<size_t>(kMaxGrid) * kRowCheckSums);
+        pkr_.reset(static_cast<size_t>(kMaxGrid) * kKktRowSums);
+        pkc_.reset(static_cast<size_t>(kMaxGrid) * kKktColSums);
     }
 
     ~HalpernEngine() override {
@@ -466,10 +503,12 @@ public:
             VK_CUDA(cudaMemsetAsync(s64_.y0.get(), 0, m * sizeof(double), s_));
         }
         HalCtl c{};
-        c.eta = eta_;
+        c.knorm = knorm_;
+        c.lq = lq_;
         c.omega = omega0_;
-        c.tau = eta_ / omega0_;
-        c.sigma = eta_ * omega0_;
+        step_params(c.knorm, c.lq, c.omega, c.eta, c.rho);
+        c.tau = c.eta / omega0_;
+        c.sigma = c.eta * omega0_;
         c.r_restart = -1.0;
         c.r_prev = std::numeric_limits<double>::infinity();
         c.bnorm = bnorm_;
@@ -617,6 +656,14 @@ private:
         for (DevBuf<T> *b : {&st.rl, &st.ru, &st.rs, &st.y, &st.y0, &st.yhat}) b->reset(mm);
         scale_vec_kernel<T><<<grid1d(n), 256, 0, s_>>>(dm_.c.get(), cs_.get(), n, 0, st.c.get());
         convert_kernel<T, double><<<grid1d(n), 256, 0, s_>>>(cs_.get(), n, st.cs.get());
+        if (dm_.qp) {
+            // Q^ = D Q D (Q symmetric, so the same column scale on both sides)
+            st.q.reset(padded(dm_.q_nnz));
+            st.qx.reset(n);
+            scale_matrix_kernel<T><<<ceil_div(int64_t(n) * 32, 256), 256, 0, s_>>>(
+                dm_.q.ro.get(), dm_.q.ci.get(), dm_.q_val.get(), cs_.get(), cs_.get(), n, false, st.q.get());
+            VK_CUDA(cudaMemsetAsync(st.qx.get(), 0, n * sizeof(T), s_));
+        }
         if (m > 0) {
             scale_vec_kernel<T><<<grid1d(m), 256, 0, s_>>>(dm_.rl.get(), rs_.get(), m, 2, st.rl.get());
             scale_vec_kernel<T><<<grid1d(m), 256, 0, s_>>>(dm_.ru.get(), rs_.get(), m, 2, st.ru.get());
@@ -666,7 +713,33 @@ private:
             }
             sigma_max = prev;
         }
-        eta_ = sigma_max > 0.0 ? 0.99 / sigma_max : 1.0;
+        knorm_ = sigma_max;
+        // lambda_max(Q^) by power iteration on Q^ (PSD), same start and stopping rule
+        lq_ = 0.0;
+        if (dm_.qp && dm_.q_nnz > 0) {
+            seed_kernel<<<grid1d(n), 256, 0, s_>>>(v.get(), n);
+            norm2(v.get(), n);
+            scal_kernel<double><<<grid1d(n), 256, 0, s_>>>(v.get(), n, nrm.get());
+            double prev = 0.0;
+            for (int it = 0; it < kPowerMax; ++it) {
+                PlainStore<double> ez;
+                ez.y = z.get();
+                launch_tiles<double, double, 1, false>(view(dm_.q, s64_.q.get()), Gathers<double, 1>{{v.get()}}, ez, s_);
+                norm2(z.get(), n);
+                double h = 0.0;
+                VK_CUDA(cudaMemcpyAsync(&h, nrm.get(), sizeof(double), cudaMemcpyDeviceToHost, s_));
+                VK_CUDA(cudaStreamSynchronize(s_));
+                const double est = std::sqrt(h); // |Q^ v| with |v| = 1
+                scal_kernel<double><<<grid1d(n), 256, 0, s_>>>(z.get(), n, nrm.get());
+                std::swap(v, z);
+                if (it > 10 && std::abs(est - prev) <= 1e-6 * est) {
+                    prev = est;
+                    break;
+                }
+                prev = est;
+            }
+            lq_ = prev;
+        }
         // |c^| and |b^| (scaled) for omega_0; |c| and |b| original for the KKT scales
         std::vector<double> hc(n), hrl(m), hru(m), hcs(n), hrs(m);
         VK_CUDA(cudaMemcpyAsync(hcs.data(), cs_.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s_));
@@ -722,6 +795,7 @@ private:
         for (int it = 0; it < chunk_; ++it) {
             const bool check = it == chunk_ - 1;
             if (check) {
+                q_pass(st, st.x.get());
                 grids.col = col_pass<T, true>(st, it);
                 grids.row = row_pass<T, true>(st, it);
                 grids.kkt_row = kkt_passes(st, grids.kkt_col);
@@ -734,6 +808,7 @@ private:
                                                                     st.yhat.get(), st.m);
                 VK_LAUNCH_CHECK();
             } else {
+                q_pass(st, st.x.get());
                 col_pass<T, false>(st, it);
                 row_pass<T, false>(st, it);
             }
@@ -749,11 +824,22 @@ private:
         return ex;
     }
 
+    // QP: qx = Q^ v (no-op for an LP, and skipped once the solve is done).
+    template <class T>
+    void q_pass(HalState<T> &st, const T *v) {
+        if (!dm_.qp) return;
+        QStore<T> e;
+        e.ctl = ctl_.get();
+        e.y = st.qx.get();
+        launch_tiles<T, T, 1, false>(view(dm_.q, st.q.get()), Gathers<T, 1>{{v}}, e, s_);
+    }
+
     template <class T, bool CHECK>
     int col_pass(HalState<T> &st, int it) {
         HalColEpi<T, CHECK> e;
         e.ctl = ctl_.get();
         e.it = it;
+        e.qx = dm_.qp ? st.qx.get() : nullptr;
         e.x = st.x.get();
         e.xbar = st.xbar.get();
         e.xhat = st.xhat.get();
@@ -794,8 +880,10 @@ private:
             r.partials = pkr_.get();
             gr = launch_tiles<T, T, 1, false>(view(dm_.a, st.ka.get()), Gathers<T, 1>{{st.xhat.get()}}, r, s_);
         }
+        q_pass(st, st.xhat.get());
         KktColEpi<T> c;
         c.ctl = ctl_.get();
+        c.qx = dm_.qp ? st.qx.get() : nullptr;
         c.xhat = st.xhat.get();
         c.c = st.c.get();
         c.l = st.l.get();
@@ -818,7 +906,7 @@ private:
     DevBuf<HalCtl> ctl_;
     HostBuf<HalCtl> hctl_;
     DevBuf<double> pc_, pr_, pkr_, pkc_;
-    double eta_ = 1.0, omega0_ = 1.0, bnorm_ = 0.0, cnorm_ = 0.0;
+    double knorm_ = 0.0, lq_ = 0.0, omega0_ = 1.0, bnorm_ = 0.0, cnorm_ = 0.0;
     cudaGraphExec_t g64_ = nullptr, g32_ = nullptr;
     long long graph_nodes_ = 0, launches_ = 0;
 };
@@ -826,7 +914,6 @@ private:
 } // namespace
 
 std::unique_ptr<Engine> make_halpern_engine(const DeviceModel &dm, const vk_options &o, cudaStream_t s) {
-    if (dm.qp) throw Unsupported("the Halpern scheme solves LPs; use VK_ALGO_REFERENCE for a QP");
     return std::make_unique<HalpernEngine>(dm, o, s);
 }
 

@@ -248,3 +248,10 @@ def workload_independent_lps(count: int = 256, seed: int = 2024, m_min: int = 50
     ms = np.exp(rng.uniform(np.log(m_min), np.log(m_max), size=count)).astype(np.int64)
     return [lp_uniform(int(m), int(2 * m), per_col, seed=seed + b, name=f"lp m={m} n={2 * m} seed={seed + b}")
             for b, m in enumerate(ms)]
+
+
+def workload_qp(seed: int = 2024) -> Instance:
+    """The large convex QP: n=500,000, m=200,000, A with 6 nonzeros per column
+    (3M), Q = D + B'B with B 50,000 x n, 4 per row, x in [-5, 5], c ~ N(0,1)."""
+    return qp_sparse(200_000, 500_000, 6, b_rows=50_000, b_per_row=4, seed=seed,
+                     name=f"qp m=2e5 n=5e5 A nnz=3M Q=D+B'B seed={seed}")
