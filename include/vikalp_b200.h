@@ -254,6 +254,45 @@ int vk_batch_solve(const vk_problem *problems, int32_t count, const vk_options *
 int vk_batch_solve_shared(const vk_problem *problem, int32_t count, const double *lower, const double *upper,
                           const double *warm, const vk_options *opts, vk_result *results);
 
+/* ---- differentiation ---------------------------------------------------------- */
+
+typedef struct {
+    double active_tolerance; /* row / bound activity: within tol * (1 + |bound|) (1e-6) */
+    double solve_tolerance;  /* LSQR stop: relative residual / normal residual (1e-10)  */
+    int64_t iteration_limit; /* LSQR iterations per instance (20000)                    */
+    int32_t device;          /* CUDA device ordinal (0)                                 */
+} vk_adjoint_options;
+
+typedef struct {
+    int64_t rows_active; /* |R|: equality rows and rows at a bound          */
+    int64_t cols_free;   /* |F|: variables strictly inside their bounds     */
+    int64_t iterations;  /* LSQR iterations                                 */
+    int32_t status;      /* VK_STATUS_OPTIMAL or VK_STATUS_ITERATION_LIMIT  */
+    double residual;     /* |A_RF' w - g_F| / |g_F|                         */
+    double normal_residual; /* |A_RF (A_RF' w - g_F)| / (|A_RF|_F |A_RF' w - g_F|) */
+} vk_adjoint_info;
+
+void vk_default_adjoint_options(vk_adjoint_options *opts);
+
+/* Gradients of L = dL_dx' x* + dL_dobj * c'x* for `count` solved LPs with
+ * respect to c, the row bounds and the stored values of A, through the
+ * active-set KKT system of each optimum (no counterpart in the reference).
+ * x / y: the optimum (as vk_pdhg_solve / vk_batch_solve return it; y > 0 is an
+ * active upper row bound), solved well below active_tolerance. Active rows R:
+ * a finite bound within active_tolerance of A x; free columns F: strictly
+ * inside both bounds. With w = the minimum-norm least-squares solution of
+ * A_RF' w = dL_dx[F] (LSQR on the GPU, all instances at once):
+ *   dL_dc[j]  = dL_dobj * x[j]
+ *   dL_db[i]  = w[i] - dL_dobj * y[i]       (b_i: the active bound of row i;
+ *                                            0 for an inactive row)
+ *   dL_dA[k]  = (-w[i] + dL_dobj * y[i]) * x[j]   (stored entry k = (i, j))
+ * All arrays are the instances' arrays concatenated in order: x, dL_dx and
+ * dL_dc hold sum(n) doubles, y and dL_db sum(m), dL_dA sum(nnz); outputs may
+ * be NULL; info is NULL or `count` records. Problems must be LPs. */
+int vk_lp_adjoint(const vk_problem *problems, int32_t count, const double *x, const double *y,
+                  const double *dL_dx, double dL_dobj, const vk_adjoint_options *opts, double *dL_dc,
+                  double *dL_db, double *dL_dA, vk_adjoint_info *info);
+
 #ifdef __cplusplus
 }
 #endif

@@ -179,3 +179,18 @@ def test_shared_batch_validates_the_model():
         vk.batch_solve_shared(M(), 4, algorithm="reference")
     assert e.value.code == vk.VK_ERR_UNSUPPORTED
     assert vk.lib().vk_batch_solve_shared(None, 1, None, None, None, None, None) == vk.VK_ERR_INVALID
+
+
+def test_adjoint_validates_before_the_device():
+    lp = M(m=1, row_offsets=np.array([0, 1], np.int64), col_idx=np.array([0], np.int64), values=np.array([1.0]),
+           row_lower=np.array([-np.inf]), row_upper=np.array([4.0]))
+    with pytest.raises(vk.VkError) as e:
+        vk.lp_adjoint([lp], [np.array([np.nan])], [np.zeros(1)], [np.ones(1)])
+    assert e.value.code == vk.VK_ERR_INVALID and e.value.msg == "x and dL_dx must be finite"
+    q = M(q_row_offsets=np.array([0, 1], np.int64), q_col_idx=np.array([0], np.int64), q_values=np.array([1.0]))
+    with pytest.raises(vk.VkError) as e:
+        vk.lp_adjoint([q], [np.zeros(1)], [np.zeros(0)], [np.ones(1)])
+    assert e.value.code == vk.VK_ERR_UNSUPPORTED
+    with pytest.raises(vk.VkError) as e:
+        vk.lp_adjoint([lp], [np.zeros(1)], [np.zeros(1)], [np.ones(1)], solve_tolerance=0.0)
+    assert e.value.code == vk.VK_ERR_INVALID

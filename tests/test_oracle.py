@@ -125,3 +125,20 @@ def test_oracle_matches_live_reference(oracle, seed):
     a = oracle.pdhg_solve(q, iteration_limit=77, primal_tolerance=0.0, dual_tolerance=0.0)
     b = ref.solve_continuous(q, qp=True, iteration_limit=77, primal_tolerance=0.0, dual_tolerance=0.0)
     assert same_bits(a["x"], b["x"]) and same_bits(a["y"], b["y"])
+
+
+def test_adjoint_oracle_against_finite_differences():
+    # the active-set KKT gradient against central differences of HiGHS re-solves
+    from oracle import adjoint
+
+    inst = synthetic.lp_uniform(120, 240, 6, seed=41)
+    x, y = adjoint.highs_solve(inst)
+    rng = np.random.default_rng(3)
+    g = rng.standard_normal(inst.n)
+    for w_obj in (0.0, 1.0):
+        gr = adjoint.kkt_gradient(inst, x, y, g, w_obj=w_obj)
+        assert gr["rows_active"] == gr["cols_free"]  # a nondegenerate vertex
+        for key, size in (("b", inst.m), ("A", inst.nnz), ("c", inst.n)):
+            d = rng.standard_normal(size)
+            fd = adjoint.fd_directional(inst, g, {key: d}, w_obj=w_obj)
+            assert abs(fd - gr[key] @ d) <= 1e-5 * max(1.0, abs(fd)), (w_obj, key)

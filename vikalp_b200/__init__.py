@@ -73,6 +73,16 @@ class Result(C.Structure):
                 ("fp32_iterations", C.c_int64), ("kernel_launches", C.c_int64), ("message", C.c_char * 256)]
 
 
+class AdjointOptions(C.Structure):
+    _fields_ = [("active_tolerance", C.c_double), ("solve_tolerance", C.c_double), ("iteration_limit", C.c_int64),
+                ("device", C.c_int32)]
+
+
+class AdjointInfo(C.Structure):
+    _fields_ = [("rows_active", C.c_int64), ("cols_free", C.c_int64), ("iterations", C.c_int64),
+                ("status", C.c_int32), ("residual", C.c_double), ("normal_residual", C.c_double)]
+
+
 # Every symbol include/vikalp_b200.h declares, with its ctypes signature.
 _SIGNATURES = {
     "vk_default_options": (None, [C.POINTER(Options)]),
@@ -96,6 +106,9 @@ _SIGNATURES = {
     "vk_batch_solve": (C.c_int, [C.POINTER(Problem), C.c_int32, C.POINTER(Options), C.POINTER(Result)]),
     "vk_batch_solve_shared": (C.c_int, [C.POINTER(Problem), C.c_int32, _f64p, _f64p, _f64p, C.POINTER(Options),
                                         C.POINTER(Result)]),
+    "vk_default_adjoint_options": (None, [C.POINTER(AdjointOptions)]),
+    "vk_lp_adjoint": (C.c_int, [C.POINTER(Problem), C.c_int32, _f64p, _f64p, _f64p, C.c_double,
+                                C.POINTER(AdjointOptions), _f64p, _f64p, _f64p, C.POINTER(AdjointInfo)]),
 }
 
 _lib = None
@@ -291,6 +304,33 @@ def batch_solve_shared(inst, count, lower=None, upper=None, warm=None, **opts) -
                    last_metric=r.last_metric, solve_seconds=r.solve_seconds, iterate_seconds=r.iterate_seconds,
                    fp32_iterations=r.fp32_iterations, kernel_launches=r.kernel_launches, message=r.message.decode())
     return outs
+
+
+def lp_adjoint(instances, xs, ys, grads, dL_dobj=0.0, **opts) -> list[dict]:
+    """Active-set adjoint of solved LPs (vk_lp_adjoint): per instance the
+    gradients {"c", "b", "A"} of L = grad'x* + dL_dobj * c'x* and the solve info."""
+    keep = _Keep()
+    probs = (Problem * len(instances))(*[problem_struct(inst, keep) for inst in instances])
+    cat = lambda arrs: np.ascontiguousarray(np.concatenate([np.asarray(a, np.float64) for a in arrs]))  # noqa: E731
+    x, y, g = cat(xs), cat(ys) if sum(i.m for i in instances) else np.zeros(1), cat(grads)
+    o = AdjointOptions()
+    lib().vk_default_adjoint_options(C.byref(o))
+    for k, v in opts.items():
+        setattr(o, k, v)
+    dc, db = np.zeros(x.size), np.zeros(max(1, sum(i.m for i in instances)))
+    nnz = [int(np.asarray(i.row_offsets)[i.m]) for i in instances]
+    da = np.zeros(max(1, sum(nnz)))
+    info = (AdjointInfo * len(instances))()
+    _check(lib().vk_lp_adjoint(probs, len(instances), _p(x), _p(y), _p(g), float(dL_dobj), C.byref(o), _p(dc),
+                               _p(db), _p(da), info))
+    out, jn, im, kz = [], 0, 0, 0
+    for inst, f, nz in zip(instances, info, nnz):
+        out.append({"c": dc[jn:jn + inst.n].copy(), "b": db[im:im + inst.m].copy(), "A": da[kz:kz + nz].copy(),
+                    "rows_active": f.rows_active, "cols_free": f.cols_free, "iterations": f.iterations,
+                    "status": STATUS.get(f.status, str(f.status)), "residual": f.residual,
+                    "normal_residual": f.normal_residual})
+        jn, im, kz = jn + inst.n, im + inst.m, kz + nz
+    return out
 
 
 def spmv(ro, ci, v, rows, cols, x, y=None, alpha=1.0, beta=0.0, transpose=False, order="fast"):

@@ -12,6 +12,7 @@
 // control kernel with one thread per instance applies the same stop / restart
 // / primal-weight rules as the single-instance engine (vk_halpern.cu). The
 // chunk of check_every iterations is one CUDA graph.
+#include "vk_blockdiag.cuh"
 #include "vk_engine.cuh"
 
 #include <algorithm>
@@ -511,52 +512,24 @@ private:
     }
 
     void concatenate(const vk_problem *probs) {
-        row_off_.assign(B_ + 1, 0);
-        col_off_.assign(B_ + 1, 0);
-        std::vector<int64_t> nnz_off(B_ + 1, 0);
-        for (int b = 0; b < B_; ++b) {
-            const vk_problem &p = probs[b];
-            row_off_[b + 1] = row_off_[b] + static_cast<int>(p.A.rows);
-            col_off_[b + 1] = col_off_[b] + static_cast<int>(p.A.cols);
-            nnz_off[b + 1] = nnz_off[b] + (p.A.rows > 0 ? p.A.row_offsets[p.A.rows] : 0);
-        }
-        m_ = row_off_[B_];
-        n_ = col_off_[B_];
-        nnz_ = nnz_off[B_];
-        h_ro_.assign(m_ + 1, 0);
-        h_ci_.resize(nnz_);
-        h_v_.resize(nnz_);
-        h_c_.resize(n_);
-        h_vl_.resize(n_);
-        h_vu_.resize(n_);
-        h_rl_.resize(m_);
-        h_ru_.resize(m_);
-        offset_.resize(B_);
-        h_rinst_.resize(m_);
-        h_cinst_.resize(n_);
-        for (int b = 0; b < B_; ++b) {
-            const vk_problem &p = probs[b];
-            const int r0 = row_off_[b], c0 = col_off_[b];
-            const int64_t k0 = nnz_off[b];
-            for (int64_t i = 0; i < p.A.rows; ++i) {
-                h_ro_[r0 + i + 1] = k0 + p.A.row_offsets[i + 1];
-                h_rinst_[r0 + i] = b;
-                h_rl_[r0 + i] = p.row_lower[i];
-                h_ru_[r0 + i] = p.row_upper[i];
-            }
-            const int64_t nz = nnz_off[b + 1] - k0;
-            for (int64_t k = 0; k < nz; ++k) {
-                h_ci_[k0 + k] = c0 + p.A.col_indices[k];
-                h_v_[k0 + k] = p.A.values[k];
-            }
-            for (int64_t j = 0; j < p.A.cols; ++j) {
-                h_c_[c0 + j] = p.c[j];
-                h_vl_[c0 + j] = p.var_lower[j];
-                h_vu_[c0 + j] = p.var_upper[j];
-                h_cinst_[c0 + j] = b;
-            }
-            offset_[b] = p.objective_offset;
-        }
+        BlockDiag bd;
+        concat_instances(probs, B_, bd);
+        m_ = bd.m;
+        n_ = bd.n;
+        nnz_ = bd.nnz;
+        row_off_ = std::move(bd.row_off);
+        col_off_ = std::move(bd.col_off);
+        h_rinst_ = std::move(bd.rinst);
+        h_cinst_ = std::move(bd.cinst);
+        h_ro_ = std::move(bd.ro);
+        h_ci_ = std::move(bd.ci);
+        h_v_ = std::move(bd.v);
+        h_c_ = std::move(bd.c);
+        h_vl_ = std::move(bd.vl);
+        h_vu_ = std::move(bd.vu);
+        h_rl_ = std::move(bd.rl);
+        h_ru_ = std::move(bd.ru);
+        offset_ = std::move(bd.offset);
         // norms in original units per instance
         bnorm_.assign(B_, 0.0);
         cnorm_.assign(B_, 0.0);
@@ -581,33 +554,37 @@ private:
     }
 
     void setup_device() {
-        // pattern with tile breaks at instance starts
-        std::vector<unsigned char> rbreak(m_ + 1, 0), cbreak(n_ + 1, 0);
-        for (int b = 0; b <= B_; ++b) {
-            rbreak[row_off_[b]] = 1;
-            cbreak[col_off_[b]] = 1;
+        // block-diagonal A and A' with instance-aligned tiles
+        {
+            BlockDiag bd;
+            bd.count = B_;
+            bd.m = m_;
+            bd.n = n_;
+            bd.nnz = nnz_;
+            bd.row_off = row_off_;
+            bd.col_off = col_off_;
+            bd.rinst = h_rinst_;
+            bd.cinst = h_cinst_;
+            bd.ro = std::move(h_ro_);
+            bd.ci = std::move(h_ci_);
+            bd.v = std::move(h_v_);
+            DeviceBlockDiag dd;
+            upload_block_diag(bd, dd, s_, true);
+            a_ = std::move(dd.a);
+            at_ = std::move(dd.at);
+            perm_ = std::move(dd.perm);
+            a_val_ = std::move(dd.a_val);
+            at_val_ = std::move(dd.at_val);
+            rinst_ = std::move(dd.rinst);
+            cinst_ = std::move(dd.cinst);
+            tinst_a_ = std::move(dd.tinst_a);
+            tinst_at_ = std::move(dd.tinst_at);
+            tbeg_a_ = std::move(dd.tbeg_a);
+            tbeg_at_ = std::move(dd.tbeg_at);
         }
-        DevBuf<unsigned char> drb, dcb;
-        up(drb, rbreak);
-        up(dcb, cbreak);
-        upload_pattern(m_, n_, h_ro_.data(), h_ci_.data(), a_, s_);
-        build_tiles(a_, s_, drb.get());
-        DevBuf<double> a_val;
-        a_val.reset(padded(nnz_));
-        if (nnz_ > 0) VK_CUDA(cudaMemcpyAsync(a_val.get(), h_v_.data(), nnz_ * sizeof(double), cudaMemcpyHostToDevice, s_));
-        transpose_pattern(a_, at_, perm_, s_);
-        build_tiles(at_, s_, dcb.get());
-        DevBuf<double> at_val(padded(nnz_));
-        gather_values<double, double>(perm_.get(), a_val.get(), at_val.get(), nnz_, s_);
-        log_.mark("upload + transpose");
-        autotune_pattern<double>(a_, a_val.get(), s_);
-        autotune_pattern<double>(at_, at_val.get(), s_);
-        log_.mark("autotune");
-        up(rinst_, h_rinst_);
-        up(cinst_, h_cinst_);
-        // instance of each tile and each instance's first tile
-        tile_instances(a_, h_rinst_, tinst_a_, tbeg_a_);
-        tile_instances(at_, h_cinst_, tinst_at_, tbeg_at_);
+        log_.mark("upload + transpose + autotune");
+        const DevBuf<double> &a_val = a_val_;
+        const DevBuf<double> &at_val = at_val_;
         DevBuf<double> c, vl, vu, rl, ru;
         up(c, h_c_);
         up(vl, h_vl_);
@@ -646,6 +623,8 @@ private:
         bscale_vec_kernel<double><<<grid1d(n_), 256, 0, s_>>>(vu.get(), cs_.get(), n_, 1, s64_.u.get());
         VK_LAUNCH_CHECK();
         step_sizes();
+        a_val_.release(); // the scaled copies carry on
+        at_val_.release();
         // control arrays
         const size_t Bs = static_cast<size_t>(B_);
         for (DevBuf<double> *d : {&eta_, &omega_, &tau_, &sigma_, &rr_, &rp_, &bn_, &cn_, &off_, &kkt_, &relp_, &reld_,
@@ -676,22 +655,6 @@ private:
         h_rel_d_.resize(B_);
         h_rel_gap_.resize(B_);
         VK_CUDA(cudaStreamSynchronize(s_));
-    }
-
-    void tile_instances(const CsrPattern32 &p, const std::vector<int> &inst, DevBuf<int> &tinst, DevBuf<int> &tbeg) {
-        std::vector<int> tiles(p.ntiles + 1);
-        VK_CUDA(cudaMemcpyAsync(tiles.data(), p.tiles.get(), tiles.size() * sizeof(int), cudaMemcpyDeviceToHost, s_));
-        VK_CUDA(cudaStreamSynchronize(s_));
-        std::vector<int> ti(std::max(p.ntiles, 1), 0), beg(B_ + 1, p.ntiles);
-        for (int t = p.ntiles - 1; t >= 0; --t) {
-            ti[t] = inst[tiles[t]];
-            beg[ti[t]] = t;
-        }
-        // instances without tiles start where the next instance starts
-        for (int b = B_ - 1; b >= 0; --b)
-            if (beg[b] > beg[b + 1]) beg[b] = beg[b + 1];
-        up(tinst, ti);
-        up(tbeg, beg);
     }
 
     template <class T>
@@ -982,6 +945,7 @@ private:
     std::vector<double> h_v_, h_c_, h_vl_, h_vu_, h_rl_, h_ru_, offset_, bnorm_, cnorm_, h_eta_, h_omega0_;
     CsrPattern32 a_, at_;
     DevBuf<int> perm_, rinst_, cinst_, tinst_a_, tinst_at_, tbeg_a_, tbeg_at_;
+    DevBuf<double> a_val_, at_val_; // original values (setup only)
     DevBuf<double> rs_, cs_;
     BState<double> s64_;
     BState<float> s32_;

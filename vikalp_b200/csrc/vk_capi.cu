@@ -391,4 +391,31 @@ int vk_batch_solve_shared(const vk_problem *problem, int32_t count, const double
     });
 }
 
+void vk_default_adjoint_options(vk_adjoint_options *o) {
+    if (!o) return;
+    o->active_tolerance = 1e-6;
+    o->solve_tolerance = 1e-10;
+    o->iteration_limit = 20000;
+    o->device = 0;
+}
+
+int vk_lp_adjoint(const vk_problem *problems, int32_t count, const double *x, const double *y, const double *dL_dx,
+                  double dL_dobj, const vk_adjoint_options *opts, double *dL_dc, double *dL_db, double *dL_dA,
+                  vk_adjoint_info *info) {
+    return guarded([&] {
+        if (!problems || count <= 0 || !x || !dL_dx) return set_error(VK_ERR_INVALID, "invalid argument");
+        int64_t m = 0;
+        for (int b = 0; b < count; ++b) m += problems[b].A.rows;
+        if (m > 0 && !y) return set_error(VK_ERR_INVALID, "y is required when the problems have rows");
+        vk_adjoint_options o;
+        if (opts)
+            o = *opts;
+        else
+            vk_default_adjoint_options(&o);
+        static const double none = 0.0;
+        vk::lp_adjoint(problems, count, x, y ? y : &none, dL_dx, dL_dobj, o, dL_dc, dL_db, dL_dA, info);
+        return VK_OK;
+    });
+}
+
 } // extern "C"

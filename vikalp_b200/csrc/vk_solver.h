@@ -74,5 +74,8 @@ void batch_solve(const vk_problem *problems, int count, const vk_options &o, vk_
 // Relaxations of one LP differing in variable bounds / warm start (vk_batch.cu).
 void batch_solve_shared(const vk_problem &p, int count, const double *lower, const double *upper,
                         const double *warm, const vk_options &o, vk_result *results);
+// Active-set adjoint of solved LPs (vk_adjoint.cu).
+void lp_adjoint(const vk_problem *probs, int count, const double *x, const double *y, const double *g, double w_obj,
+                const vk_adjoint_options &o, double *dc, double *db, double *da, vk_adjoint_info *info);
 
 } // namespace vk
