@@ -21,6 +21,9 @@ replicas, no collective on the path). The same line carries:
   batched        768 LPs (512 shared-matrix node relaxations + 256 independent
                  LPs) to 1e-6 relative KKT in two batches, mixed and fp64, vs
                  the plain fp64 engine one instance at a time (sampled)
+  adjoint        256 LPs solved and differentiated (gradients w.r.t. b and A)
+                 in batches, errors against the CPU FP64 KKT gradient
+  time_to_tol.qp the convex QP (n=5e5, m=2e5), fp64 vs mixed
   roofline       the sparse-pass kernel against measured HBM bandwidth
   cpu_baseline   the reference's CPU implementation on this host
 `python bench.py --impl reference` times the reference's own CPU PDHG
@@ -194,8 +197,8 @@ def batched_figures(sample_every=64):
     """The batched workload: 512 node relaxations of one LP (m=50,000, n=100,000,
     6 nonzeros per column, 1-12 tightened variables each) and 256 independent
     LPs (m log-uniform on [500, 20000], n=2m, 8 per column), all to 1e-6
-    relative KKT. Both batches run at once (two host threads, two streams);
-    wall time from host arrays to results. The plain-FP64 comparison solves
+    relative KKT. The two batches run one after the other; wall time from
+    host arrays to results. The plain-FP64 comparison solves
     instances one by one with the single-instance float64 engine (a resident
     model for the nodes, create+solve for each independent LP) on a systematic
     sample (every `sample_every`-th node, every (sample_every/2)-th LP) and
@@ -220,12 +223,11 @@ def batched_figures(sample_every=64):
             res["indep"] = vk.batch_solve(indep, precision=prec, **tol)
             res["indep_s"] = time.perf_counter() - t
 
+        # one after the other: run concurrently, each batch's setup (device
+        # allocation and release) waits on the other's iterations
         t0 = time.perf_counter()
-        th = [threading.Thread(target=shared), threading.Thread(target=independent)]
-        for t in th:
-            t.start()
-        for t in th:
-            t.join()
+        shared()
+        independent()
         wall = time.perf_counter() - t0
         rs = res["shared"] + res["indep"]
         status = {}
@@ -258,6 +260,43 @@ def batched_figures(sample_every=64):
                                     "sample": f"{len(node_t)} of 512 nodes, {len(indep_t)} of 256 LPs, mean x count"}
     out["speedup_mixed_batched_vs_plain_fp64"] = round(est / out["mixed"]["wall_s"], 2)
     return out
+
+
+def adjoint_figures(count=256, checked=3):
+    """The differentiable-LP workload: `count` LPs (m=1000, n=2000, 8 nonzeros
+    per column, distinct seeds), solved in one batch (mixed precision, float64
+    polish to 1e-9 relative KKT), then gradients of L = g'x* (g ~ N(0,1)) with
+    respect to b and the values of A in one adjoint batch. Errors: relative
+    2-norm against the CPU FP64 active-set gradient at HiGHS's optimum on the
+    first `checked` instances."""
+    import vikalp_b200 as vk
+    from oracle import adjoint as oadj
+    from vikalp_b200 import synthetic
+    lps = [synthetic.lp_uniform(1000, 2000, 8, seed=7000 + s) for s in range(count)]
+    rng = np.random.default_rng(99)
+    gs = [rng.standard_normal(i.n) for i in lps]
+    t0 = time.perf_counter()
+    sols = vk.batch_solve(lps, precision="mixed", iteration_limit=500000, relative_tolerance=1e-9,
+                          time_limit_seconds=300)
+    t_solve = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    grads = vk.lp_adjoint(lps, [s["x"] for s in sols], [s["y"] for s in sols], gs)
+    t_adj = time.perf_counter() - t0
+    errs = {"b": [], "A": []}
+    for k in range(checked):
+        x, y = oadj.highs_solve(lps[k])
+        want = oadj.kkt_gradient(lps[k], x, y, gs[k])
+        for key in errs:
+            errs[key].append(float(np.linalg.norm(grads[k][key] - want[key]) / np.linalg.norm(want[key])))
+    status = {}
+    for s in sols:
+        status[s["status"]] = status.get(s["status"], 0) + 1
+    return {"workload": f"{count} LPs m=1000 n=2000 nnz=16k (distinct seeds), L = g'x*, g ~ N(0,1)",
+            "solve_s": round(t_solve, 3), "solve_status": status, "adjoint_s": round(t_adj, 3),
+            "adjoint_max_lsqr_iterations": int(max(g["iterations"] for g in grads)),
+            "adjoint_status": sorted({g["status"] for g in grads}),
+            "max_rel_err_vs_cpu_fp64_kkt": {k: max(v) for k, v in errs.items()},
+            "checked_instances": checked}
 
 
 def reference_cpu_rate(inst, budget_s):
@@ -382,6 +421,9 @@ def main():
         line["time_to_tol"] = ttt
         if not args.no_batched:
             line["batched"] = batched_figures()
+            line["adjoint"] = adjoint_figures()
+            line["time_to_tol"]["qp"] = time_to_tolerance(synthetic.workload_qp(), "qp m=2e5 n=5e5 A nnz=3M Q nnz=1.1M",
+                                                          400000, time_limit=120)
         if ws == 1:
             rate, n_it, secs = reference_cpu_rate(inst, budget_s=20.0)
             line["cpu_baseline"] = {"value": round(rate, 4), "unit": "iter/s", "cores": 1, "kind": "reference",
