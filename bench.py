@@ -402,7 +402,8 @@ def main():
         achieved = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9
         line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                             "frac": round(achieved / peak, 4), "traffic": profile_traffic(),
-                            "kernel": "tile_kernel_fast (sparse pass, A x, fp64)",
+                            "kernel": f"sparse pass A x fp64, autotuned variant {dom['variant']} "
+                                      f"({'sub-warp tile_kernel_sub' if dom['variant'] >= 5 else 'segmented-scan tile_kernel_fast'})",
                             "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                             "algorithmic_bytes": dom["bytes"], "ms": dom["ms"]}
         line["spmv"] = sp

@@ -125,8 +125,8 @@ def test_spmat_device_apply(oracle):
     assert np.all(np.abs(y32.cpu().numpy() - want) <= 1e-5 * (mass + 1e-30))
     assert A.bytes() == len(ci) * 12 + 4 * (m + 1) + 8 * n + 8 * m
     # every kernel variant the autotuner chooses from gives the same product
-    assert 0 <= A.variant() < 5 and 0 <= A.variant(True) < 5
-    for var in range(5):
+    assert 0 <= A.variant() < vk.FAST_VARIANTS and 0 <= A.variant(True) < vk.FAST_VARIANTS
+    for var in range(vk.FAST_VARIANTS):
         A.set_variant(var)
         y.zero_()
         A.apply(x.data_ptr(), y.data_ptr(), False, torch.cuda.current_stream().cuda_stream)
@@ -138,4 +138,4 @@ def test_spmat_device_apply(oracle):
         torch.cuda.synchronize()
         assert np.max(np.abs(yt.cpu().numpy() - want_t)) <= 1e-12 * np.abs(want_t).max(), var
     with pytest.raises(vk.VkError):
-        A.set_variant(5)
+        A.set_variant(vk.FAST_VARIANTS)

@@ -37,6 +37,9 @@ _i64p = C.POINTER(C.c_int64)
 _f64p = C.POINTER(C.c_double)
 
 
+FAST_VARIANTS = 8  # kernel variants of the sparse pass (vk_spmat_set_variant)
+
+
 class VkError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"[{code}] {msg}")

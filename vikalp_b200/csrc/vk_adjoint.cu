@@ -145,6 +145,7 @@ struct AdjColEpi : EpiBase<double> {
         double f, u;
         int b;
     };
+    static constexpr bool kSkipTiles = true;
     __device__ bool skip_tile(int t) const { return c.done[tile_inst[t]] != 0; }
     __device__ Pre load(int j) const { return Pre{fmask[j], ubar[j], inst[j]}; }
     __device__ void row_pre(int j, const double (&s)[1], const Pre &p, double (&red)[1]) const {
@@ -184,6 +185,7 @@ struct AdjRowEpi : EpiBase<double> {
         double r, v;
         int b;
     };
+    static constexpr bool kSkipTiles = true;
     __device__ bool skip_tile(int t) const { return c.done[tile_inst[t]] != 0; }
     __device__ Pre load(int i) const { return Pre{rmask[i], vbar[i], inst[i]}; }
     __device__ void row_pre(int i, const double (&s)[1], const Pre &p, double (&red)[1]) const {

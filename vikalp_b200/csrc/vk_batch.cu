@@ -57,6 +57,7 @@ struct BColEpi : EpiBase<T> {
         T x, x0, c, l, u;
         int b;
     };
+    static constexpr bool kSkipTiles = true;
     __device__ bool skip_tile(int t) const { return ctl.done[tile_inst[t]] != 0; }
     __device__ Pre load(int j) const { return Pre{x[j], x0[j], c[j], l[j], u[j], inst[j]}; }
     __device__ void row_pre(int j, const T (&s)[1], const Pre &p, double (&red)[NR]) const {
@@ -93,6 +94,7 @@ struct BRowEpi : EpiBase<T> {
         T y, y0, rl, ru;
         int b;
     };
+    static constexpr bool kSkipTiles = true;
     __device__ bool skip_tile(int t) const { return ctl.done[tile_inst[t]] != 0; }
     __device__ Pre load(int i) const { return Pre{y[i], y0[i], rl[i], ru[i], inst[i]}; }
     __device__ void row_pre(int i, const T (&s)[1], const Pre &p, double (&red)[NR]) const {
@@ -126,6 +128,7 @@ struct BKktRowEpi : EpiBase<T> {
     struct Pre {
         T y, rl, ru, r;
     };
+    static constexpr bool kSkipTiles = true;
     __device__ bool skip_tile(int t) const { return ctl.done[tile_inst[t]] != 0; }
     __device__ Pre load(int i) const { return Pre{yhat[i], rl[i], ru[i], rs[i]}; }
     __device__ void row_pre(int, const T (&s)[1], const Pre &p, double (&red)[NR]) const {
@@ -159,6 +162,7 @@ struct BKktColEpi : EpiBase<T> {
     struct Pre {
         T x, c, l, u, d;
     };
+    static constexpr bool kSkipTiles = true;
     __device__ bool skip_tile(int t) const { return ctl.done[tile_inst[t]] != 0; }
     __device__ Pre load(int j) const { return Pre{xhat[j], c[j], l[j], u[j], cs[j]}; }
     __device__ void row_pre(int, const T (&s)[1], const Pre &p, double (&red)[NR]) const {

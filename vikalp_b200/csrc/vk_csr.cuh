@@ -108,18 +108,27 @@ struct Gathers {
 // does the CTA-level reduction itself (scratch: 32*8 doubles of shared memory).
 
 // Kernel variants of the FAST pass (the autotuner picks one per matrix):
-//   U     32-nonzero steps per load batch (loads in flight per lane)
+//   SUB   0: the warp streams the tile's nonzeros 32 at a time and forms row
+//         sums with a segmented scan (tile_kernel_fast);
+//         L > 0: sub-warps of L lanes take one row each, 32/L rows per warp
+//         step, and reduce with L-wide shuffles (tile_kernel_sub)
+//   U     loads in flight per lane (32-nonzero steps, or L-strided steps)
 //   PIPE  prefetch the next batch's indices / values while the current batch
-//         gathers and reduces
+//         gathers and reduces (SUB = 0 only)
 //   MINB  resident CTAs per SM the register allocation is held to
 struct FastVariant {
-    int u, pipe, minb;
+    int u, pipe, minb, sub;
 };
-constexpr int kFastVariants = 5;
+constexpr int kFastVariants = 8;
 __host__ __device__ constexpr FastVariant fast_variant(int v) {
-    return v == 0 ? FastVariant{4, 1, 12}
-                  : v == 1 ? FastVariant{8, 1, 8}
-                           : v == 2 ? FastVariant{8, 0, 12} : v == 3 ? FastVariant{16, 0, 8} : FastVariant{2, 1, 16};
+    return v == 0   ? FastVariant{4, 1, 12, 0}
+           : v == 1 ? FastVariant{8, 1, 8, 0}
+           : v == 2 ? FastVariant{8, 0, 12, 0}
+           : v == 3 ? FastVariant{16, 0, 8, 0}
+           : v == 4 ? FastVariant{2, 1, 16, 0}
+           : v == 5 ? FastVariant{2, 0, 12, 8}
+           : v == 6 ? FastVariant{4, 0, 12, 4}
+                    : FastVariant{2, 0, 12, 16};
 }
 
 template <class T, class A, int NV, class Epi, int U, bool PIPE, int MINB>
@@ -315,6 +324,151 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     epi.finish(red, scratch, blockIdx.x);
 }
 
+// Sub-warp variant: within a row-aligned tile, sub-warps of L lanes take one
+// row each (32/L rows per warp step); the lanes of a sub-warp stride through
+// the row's nonzeros U at a time and reduce with L-wide shuffles; lane 0 of
+// the sub-warp runs the epilogue. Rows of a multi-row tile are short
+// (<= kShortMax), so no segmented scan and no shared-memory prologue is
+// needed; a single-row tile (a long row) is streamed by the whole warp. Same
+// tile schedule, grid and epilogue interface as tile_kernel_fast.
+template <class T, class A, int NV, class Epi, int L, int U, int MINB>
+__global__ void __launch_bounds__(kTileThreads, MINB)
+    tile_kernel_sub(CsrView<T> M, Gathers<T, NV> g, Epi epi) {
+    static_assert(L == 2 || L == 4 || L == 8 || L == 16 || L == 32, "sub-warp width");
+    if (epi.skip()) return;
+    constexpr int NR = Epi::NR;
+    constexpr int G = 32 / L;
+    using Pre = typename Epi::Pre;
+    __shared__ double scratch[32 * 8];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int sl = lane % L, sw = lane / L;
+    double red[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) red[r] = 0.0;
+    A gs[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) gs[q] = epi.gscale(q);
+
+    // One long row (a single-row tile), streamed by the whole warp.
+    auto long_row = [&](int r0, int k0, int k1) {
+        const Pre pre = epi.load(r0);
+        A part[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) part[q] = A(0);
+        for (int kb = k0; kb < k1; kb += 32 * U) {
+            int c[U];
+            T v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int k = kb + 32 * u + lane;
+                c[u] = k < k1 ? __ldg(M.ci + k) : 0;
+                v[u] = k < k1 ? __ldg(M.val + k) : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (kb + 32 * u + lane < k1) {
+#pragma unroll
+                    for (int q = 0; q < NV; ++q)
+                        part[q] += static_cast<A>(v[u]) * (gs[q] * static_cast<A>(__ldg(g.p[q] + c[u])));
+                }
+            }
+        }
+        A sum[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) sum[q] = epi.init(r0, q) + warp_sum(part[q]);
+        if (lane == 0) epi.row_pre(r0, sum, pre, red);
+    };
+    // Short rows [r0, r1): G rows per warp step, one per sub-warp.
+    auto short_rows = [&](int r0, int r1) {
+        for (int rb = r0; rb < r1; rb += G) {
+            const int r = rb + sw;
+            const bool valid = r < r1;
+            int a = 0, b = 0;
+            if (valid) {
+                a = __ldg(M.ro + r);
+                b = __ldg(M.ro + r + 1);
+            }
+            Pre pre{};
+            if (valid && sl == 0) pre = epi.load(r);
+            A part[NV];
+#pragma unroll
+            for (int q = 0; q < NV; ++q) part[q] = A(0);
+            int k = a + sl;
+            for (; k + (U - 1) * L < b; k += U * L) {
+                int c[U];
+                T v[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    c[u] = __ldg(M.ci + k + u * L);
+                    v[u] = __ldg(M.val + k + u * L);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+#pragma unroll
+                    for (int q = 0; q < NV; ++q)
+                        part[q] += static_cast<A>(v[u]) * (gs[q] * static_cast<A>(__ldg(g.p[q] + c[u])));
+            }
+            for (; k < b; k += L) {
+                const int c = __ldg(M.ci + k);
+                const A v = static_cast<A>(__ldg(M.val + k));
+#pragma unroll
+                for (int q = 0; q < NV; ++q) part[q] += v * (gs[q] * static_cast<A>(__ldg(g.p[q] + c)));
+            }
+#pragma unroll
+            for (int o = L / 2; o > 0; o >>= 1)
+#pragma unroll
+                for (int q = 0; q < NV; ++q) part[q] += __shfl_xor_sync(FULL, part[q], o, L);
+            if (valid && sl == 0) {
+                A sum[NV];
+#pragma unroll
+                for (int q = 0; q < NV; ++q) sum[q] = epi.init(r, q) + part[q];
+                epi.row_pre(r, sum, pre, red);
+            }
+        }
+    };
+
+    if constexpr (Epi::kPerTile || Epi::kSkipTiles) {
+        // Tile by tile (round robin): per-tile sums and skipped tiles.
+        for (int tile = blockIdx.x * kWarps + warp; tile < M.ntiles; tile += gridDim.x * kWarps) {
+            if (epi.skip_tile(tile)) continue;
+            const int r0 = __ldg(M.tiles + tile), r1 = __ldg(M.tiles + tile + 1);
+            const int k0 = __ldg(M.tile_k + tile), k1 = __ldg(M.tile_k + tile + 1);
+            if (k1 - k0 > kCap)
+                long_row(r0, k0, k1);
+            else
+                short_rows(r0, r1);
+            if constexpr (Epi::kPerTile) {
+#pragma unroll
+                for (int r = 0; r < NR; ++r) red[r] = warp_sum(red[r]);
+                if (lane == 0) epi.tile_done(tile, red);
+#pragma unroll
+                for (int r = 0; r < NR; ++r) red[r] = 0.0;
+            }
+        }
+    } else {
+        // A contiguous range of tiles per warp; consecutive short-row tiles
+        // form one row span, so sub-warp steps are only partial at span ends.
+        const long long W = static_cast<long long>(gridDim.x) * kWarps;
+        const long long wid = static_cast<long long>(blockIdx.x) * kWarps + warp;
+        const int ta = static_cast<int>(M.ntiles * wid / W), tb = static_cast<int>(M.ntiles * (wid + 1) / W);
+        int t = ta;
+        while (t < tb) {
+            const int k0 = __ldg(M.tile_k + t), k1 = __ldg(M.tile_k + t + 1);
+            if (k1 - k0 > kCap) {
+                long_row(__ldg(M.tiles + t), k0, k1);
+                ++t;
+                continue;
+            }
+            int te = t + 1;
+            while (te < tb && __ldg(M.tile_k + te + 1) - __ldg(M.tile_k + te) <= kCap) ++te;
+            short_rows(__ldg(M.tiles + t), __ldg(M.tiles + te));
+            t = te;
+        }
+    }
+    epi.finish(red, scratch, blockIdx.x);
+}
+
 // Parity kernel: one thread per row, the reference's left-to-right order.
 template <class T, class A, int NV, class Epi>
 __global__ void __launch_bounds__(kTileThreads)
@@ -359,7 +513,11 @@ inline int resident_grid(K kernel) {
 template <class T, class A, int NV, class Epi, int V>
 inline int launch_fast(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi &epi, cudaStream_t s) {
     constexpr FastVariant fv = fast_variant(V);
-    auto kernel = tile_kernel_fast<T, A, NV, Epi, fv.u, fv.pipe != 0, fv.minb>;
+    void (*kernel)(CsrView<T>, Gathers<T, NV>, Epi);
+    if constexpr (fv.sub > 0)
+        kernel = tile_kernel_sub<T, A, NV, Epi, (fv.sub > 0 ? fv.sub : 32), fv.u, fv.minb>;
+    else
+        kernel = tile_kernel_fast<T, A, NV, Epi, fv.u, fv.pipe != 0, fv.minb>;
     static const int resident = resident_grid(kernel);
     const int need = (M.ntiles + kWarps - 1) / kWarps;
     const int grid = need < resident ? (need > 0 ? need : 1) : resident;
@@ -388,6 +546,9 @@ inline int launch_tiles(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi 
     case 2: return launch_fast<T, A, NV, Epi, 2>(M, g, epi, s);
     case 3: return launch_fast<T, A, NV, Epi, 3>(M, g, epi, s);
     case 4: return launch_fast<T, A, NV, Epi, 4>(M, g, epi, s);
+    case 5: return launch_fast<T, A, NV, Epi, 5>(M, g, epi, s);
+    case 6: return launch_fast<T, A, NV, Epi, 6>(M, g, epi, s);
+    case 7: return launch_fast<T, A, NV, Epi, 7>(M, g, epi, s);
     default: return launch_fast<T, A, NV, Epi, 0>(M, g, epi, s);
     }
 }
@@ -402,6 +563,7 @@ struct EpiBase {
     // passed to tile_done(tile, red) (FAST order only); skip_tile(tile) lets
     // a pass leave whole tiles untouched.
     static constexpr bool kPerTile = false;
+    static constexpr bool kSkipTiles = false; // true when skip_tile is overridden
     struct Pre {};
     __device__ Pre load(int) const { return Pre{}; }
     __device__ A init(int, int) const { return A(0); }
