@@ -136,8 +136,8 @@ def allmax(dist, v, local):
 
 
 def profile_traffic():
-    """DRAM bytes per launch of the sparse-pass kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "spmv_large_lp.md")
+    """DRAM bytes per launch of the dominant kernel (the row pass) from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "row_pass_large_lp.md")
     if not os.path.exists(p):
         return None
     m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
@@ -325,9 +325,13 @@ def main():
     ap.add_argument("--profile-spmv", choices=["fp64", "fp32"], default=None,
                     help="only run the sparse-product kernel 5 times on the large LP (for ncu captures)")
     ap.add_argument("--transpose", action="store_true", help="with --profile-spmv: A'y instead of A x")
+    ap.add_argument("--profile-iter", type=int, default=0,
+                    help="only run this many reference-scheme iterations on the large LP (for ncu captures)")
     args = ap.parse_args()
     if args.profile_spmv:
         return profile_spmv(args.profile_spmv, args.transpose)
+    if args.profile_iter:
+        return profile_iterations(args.profile_iter)
     K, W = max(1, args.steps), max(3, args.warmup)
     ws, rank, local, dist = dist_setup(args.gpus)
     from vikalp_b200 import synthetic
@@ -377,6 +381,9 @@ def main():
     value = ws * iters / t_dev
     ms_per_step = t_dev / (iters / CHUNK) * 1e3
     launches = r["kernel_launches"]
+    # per-kernel device times of the same passes on the same handle (eager
+    # launches with CUDA events on the solver's stream, right after the timed region)
+    prof = h.profile(2 * CHUNK) if rank == 0 else None
     h.close()
     # ---- e2e: through the C ABI from host arrays ---------------------------------
     barrier(dist)
@@ -395,17 +402,21 @@ def main():
             "warmup": W, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
             "clocks": clk.summary(), "e2e": e2e, "gpu_launches": int(launches)}
-    if rank == 0 and not args.no_extras:
+    if rank == 0:
         peak, peak_kind = measured_peaks()
-        sp = spmv_figures(inst, torch, stream)
-        dom = sp["fp64_A_x"]
+        total = sum(p["ms"] * p["launches"] for p in prof)
+        dom = max(prof, key=lambda p: p["ms"] * p["launches"])
         achieved = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9
         line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                             "frac": round(achieved / peak, 4), "traffic": profile_traffic(),
-                            "kernel": f"sparse pass A x fp64, autotuned variant {dom['variant']} "
-                                      f"({'sub-warp tile_kernel_sub' if dom['variant'] >= 5 else 'segmented-scan tile_kernel_fast'})",
+                            "kernel": f"{dom['name']} of the reference-scheme iteration (fp64, FAST order)",
                             "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                            "algorithmic_bytes": dom["bytes"], "ms": dom["ms"]}
+                            "algorithmic_bytes": int(dom["bytes"]), "ms": round(dom["ms"], 4),
+                            "passes": [{"kernel": p["name"], "ms": round(p["ms"], 4), "share": round(p["ms"] * p["launches"] / total, 3),
+                                        "gbs": round(p["bytes"] / (p["ms"] * 1e-3) / 1e9, 1) if p["bytes"] else None}
+                                       for p in prof]}
+    if rank == 0 and not args.no_extras:
+        sp = spmv_figures(inst, torch, stream)
         line["spmv"] = sp
         # Halpern scheme iteration rate (fp64 and mixed)
         hal = {}
@@ -435,6 +446,20 @@ def main():
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+    return 0
+
+
+def profile_iterations(iterations):
+    """`iterations` reference-scheme iterations (fp64, FAST order) on the large LP, for ncu captures."""
+    import torch
+
+    import vikalp_b200 as vk
+    from vikalp_b200 import synthetic
+    inst = synthetic.workload_large_lp()
+    with vk.Pdhg(inst, algorithm="reference", check_every=CHUNK) as h:
+        r = h.solve(iteration_limit=iterations, primal_tolerance=0.0, dual_tolerance=0.0, duals=False)
+    torch.cuda.synchronize()
+    print(f"ok iterations={r['iterations']} status={r['status']}")
     return 0
 
 

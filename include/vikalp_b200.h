@@ -160,6 +160,23 @@ int vk_pdhg_set_options(vk_pdhg *h, const vk_options *opts);
 
 void vk_pdhg_destroy(vk_pdhg *h);
 
+/* Device time of each kernel kind of a handle's iteration loop: runs
+ * `iterations` iterations of the handle's scheme from a cold start with the
+ * model's bounds (no tolerance stop), launched one by one instead of as a
+ * CUDA graph, with CUDA events around every kernel kind on the handle's
+ * stream. For measurement only (no counterpart in the reference, whose
+ * backend calls are timed by nothing). VK_ALGO_REFERENCE handles report
+ * three kinds: the column pass, the control (+ primal) kernels and the row
+ * pass; other schemes return VK_ERR_UNSUPPORTED. */
+typedef struct {
+    int32_t count;             /* kernel kinds reported (<= 8)                  */
+    char name[8][48];
+    double ms_per_launch[8];   /* mean device time per launch                   */
+    int64_t launches[8];
+    double bytes_per_launch[8]; /* algorithmic bytes one launch moves (0: none) */
+} vk_pass_profile;
+int vk_pdhg_profile(vk_pdhg *h, int64_t iterations, vk_pass_profile *out);
+
 /* ---- primitives (ExecutionBackend-level, ExecutionBackend.hpp:36-64) ------ */
 
 /* CSR transpose on the GPU by a stable counting sort on the column index, so
@@ -190,7 +207,7 @@ int vk_spmat_apply_device(vk_spmat *m, const void *x_device, void *y_device, int
 int64_t vk_spmat_bytes(const vk_spmat *m, int transpose);
 /* Kernel variant the setup autotuner picked for A (transpose == 0) or A'
  * (timing each candidate on this matrix), and a way to pin one
- * (0 <= variant < 8). Results agree to rounding across variants. */
+ * (0 <= variant < 11). Results agree to rounding across variants. */
 int vk_spmat_variant(const vk_spmat *m, int transpose);
 int vk_spmat_set_variant(vk_spmat *m, int transpose, int variant);
 void vk_spmat_destroy(vk_spmat *m);

@@ -63,6 +63,57 @@ def test_larger_instance_against_oracle(oracle):
         assert same_bits(got["objective"], want["objective"])
 
 
+@pytest.mark.parametrize("seed", [31, 32])
+def test_fast_order_against_oracle_through_policy_iterations(oracle, seed):
+    # The FAST order extrapolates K xbar = 2 K x+ - K x and does the primal
+    # step in the column pass except on the every-50th control step; 157 and
+    # 331 iterations cross several step-rule decisions and graph boundaries.
+    # Every iterate must stay within 1e-9 (relative to the largest |x|, |y|)
+    # of the oracle's, with the same step-rule restarts.
+    inst = synthetic.lp_powerlaw(3000, 8000, 120000, seed=seed)
+    for it in (1, 2, 51, 52, 157, 331):
+        want = oracle.pdhg_solve(inst, iteration_limit=it, primal_tolerance=0.0, dual_tolerance=0.0)
+        got = vk.solve(inst, algorithm="reference", spmv_order="fast", iteration_limit=it,
+                       primal_tolerance=0.0, dual_tolerance=0.0)
+        assert got["iterations"] == want["iterations"] == it
+        assert got["restarts"] == want["restarts"]
+        sx = 1.0 + np.abs(want["x"]).max()
+        sy = 1.0 + np.abs(want["y"]).max()
+        assert np.max(np.abs(got["x"] - want["x"])) <= 1e-9 * sx, it
+        assert np.max(np.abs(got["y"] - want["y"])) <= 1e-9 * sy, it
+
+
+def test_fast_order_tolerance_stop_matches_reference(golden_cases):
+    # the reference run that stops on its absolute metric (and is then
+    # downgraded by the original-coordinate check): the FAST order stops on
+    # the same iteration with the same status
+    case = golden_cases["lp_tol_stop"]
+    res = run(case, "fast")
+    out = case.out
+    assert res["status"] == out["status"]
+    assert abs(res["iterations"] - int(out["iterations"])) <= 1
+    assert abs(res["objective"] - out["objective"]) <= 1e-6 * (1 + abs(out["objective"]))
+
+
+@pytest.mark.parametrize("order", ["fast", "sequential"])
+def test_pass_profile(order):
+    inst = synthetic.lp_powerlaw(20000, 50000, 400000, seed=5)
+    with vk.Pdhg(inst, algorithm="reference", spmv_order=order) as h:
+        prof = h.profile(60)
+        r = h.solve(iteration_limit=300, primal_tolerance=0.0, dual_tolerance=0.0)
+    assert [p["launches"] for p in prof] == [60, 60, 60]
+    assert all(p["ms"] > 0 for p in prof)
+    nnz = inst.nnz
+    assert prof[0]["bytes"] >= 12 * nnz and prof[2]["bytes"] >= 12 * nnz
+    # the profiled passes account for the graph-launched iteration within 2x
+    per_iter = sum(p["ms"] for p in prof) * 1e-3
+    assert 0.5 * per_iter <= r["iterate_seconds"] / 300 <= 2.0 * per_iter
+    with vk.Pdhg(inst, algorithm="halpern") as h:
+        with pytest.raises(vk.VkError) as e:
+            h.profile(4)
+        assert e.value.code == vk.VK_ERR_UNSUPPORTED
+
+
 def test_repeated_solves_on_one_handle(golden_cases):
     # one device model, several solves with different overrides (the
     # branch-and-bound pattern, RelaxationOracle.hpp:17-22)

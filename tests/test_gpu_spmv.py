@@ -139,3 +139,49 @@ def test_spmat_device_apply(oracle):
         assert np.max(np.abs(yt.cpu().numpy() - want_t)) <= 1e-12 * np.abs(want_t).max(), var
     with pytest.raises(vk.VkError):
         A.set_variant(vk.FAST_VARIANTS)
+
+
+def _mostly_unit_rows(seed):
+    # 5000 rows: most with one nonzero, some with 2-40, a few of 300, one of
+    # 5000 and a few empty ones -- the mix a power-law column degree leaves
+    # in A' (every hybrid-kernel path: lane-owned rows, sub-warp rows,
+    # whole-warp rows)
+    rng = np.random.default_rng(seed)
+    n = 8000
+    lens = np.ones(5000, dtype=np.int64)
+    pick = rng.choice(5000, size=900, replace=False)
+    lens[pick[:600]] = rng.integers(2, 41, size=600)
+    lens[pick[600:640]] = 300
+    lens[pick[640]] = 5000
+    lens[pick[641:700]] = 0
+    ro = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    ci = np.concatenate([np.sort(rng.choice(n, size=k, replace=False)) for k in lens if k > 0]).astype(np.int64)
+    v = rng.standard_normal(len(ci))
+    return ro, ci, v, len(lens), n
+
+
+@pytest.mark.parametrize("make", [_with_long_rows, _mostly_unit_rows])
+def test_every_variant_on_ragged_rows(oracle, make):
+    torch = pytest.importorskip("torch")
+    ro, ci, v, m, n = make(5)
+    A = vk.SpMat(ro, ci, v, m, n, "fp64")
+    rng = np.random.default_rng(11)
+    xh, xth = rng.standard_normal(n), rng.standard_normal(m)
+    x = torch.tensor(xh, device="cuda")
+    xt = torch.tensor(xth, device="cuda")
+    want = oracle.spmv(ro, ci, v, xh)
+    want_t = oracle.spmv_t(ro, ci, v, n, xth)
+    mass = oracle.spmv(ro, ci, np.abs(v), np.abs(xh)) + 1e-300
+    mass_t = oracle.spmv_t(ro, ci, np.abs(v), n, np.abs(xth)) + 1e-300
+    s = torch.cuda.current_stream().cuda_stream
+    for var in range(vk.FAST_VARIANTS):
+        A.set_variant(var)
+        A.set_variant(var, True)
+        y = torch.full((m,), np.nan, dtype=torch.float64, device="cuda")
+        yt = torch.full((n,), np.nan, dtype=torch.float64, device="cuda")
+        A.apply(x.data_ptr(), y.data_ptr(), False, s)
+        A.apply(xt.data_ptr(), yt.data_ptr(), True, s)
+        torch.cuda.synchronize()
+        # every row written (empty rows as 0), each within 1e-13 of its absolute mass
+        assert np.all(np.abs(y.cpu().numpy() - want) <= 1e-13 * mass), var
+        assert np.all(np.abs(yt.cpu().numpy() - want_t) <= 1e-13 * mass_t), var

@@ -37,7 +37,7 @@ _i64p = C.POINTER(C.c_int64)
 _f64p = C.POINTER(C.c_double)
 
 
-FAST_VARIANTS = 8  # kernel variants of the sparse pass (vk_spmat_set_variant)
+FAST_VARIANTS = 11  # kernel variants of the sparse pass (vk_spmat_set_variant)
 
 
 class VkError(RuntimeError):
@@ -76,6 +76,11 @@ class Result(C.Structure):
                 ("fp32_iterations", C.c_int64), ("kernel_launches", C.c_int64), ("message", C.c_char * 256)]
 
 
+class PassProfile(C.Structure):
+    _fields_ = [("count", C.c_int32), ("name", (C.c_char * 48) * 8), ("ms_per_launch", C.c_double * 8),
+                ("launches", C.c_int64 * 8), ("bytes_per_launch", C.c_double * 8)]
+
+
 class AdjointOptions(C.Structure):
     _fields_ = [("active_tolerance", C.c_double), ("solve_tolerance", C.c_double), ("iteration_limit", C.c_int64),
                 ("device", C.c_int32)]
@@ -95,6 +100,7 @@ _SIGNATURES = {
     "vk_pdhg_solve": (C.c_int, [C.c_void_p, _f64p, _f64p, _f64p, C.POINTER(Result)]),
     "vk_pdhg_set_options": (C.c_int, [C.c_void_p, C.POINTER(Options)]),
     "vk_pdhg_destroy": (None, [C.c_void_p]),
+    "vk_pdhg_profile": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(PassProfile)]),
     "vk_csr_transpose": (C.c_int, [C.POINTER(Csr), _i64p, _i64p, _f64p, _i64p]),
     "vk_spmv": (C.c_int, [C.POINTER(Csr), C.c_double, _f64p, C.c_double, _f64p, C.c_int, C.c_int]),
     "vk_spmat_create": (C.c_int, [C.POINTER(Csr), C.c_int32, C.POINTER(C.c_void_p)]),
@@ -237,6 +243,13 @@ class Pdhg:
                    fp32_iterations=r.fp32_iterations, kernel_launches=r.kernel_launches,
                    message=r.message.decode())
         return out
+
+    def profile(self, iterations: int) -> list[dict]:
+        """Per-kernel-kind device times of `iterations` eager iterations (vk_pdhg_profile)."""
+        pp = PassProfile()
+        _check(lib().vk_pdhg_profile(self._h, int(iterations), C.byref(pp)))
+        return [{"name": pp.name[q].value.decode(), "ms": pp.ms_per_launch[q], "launches": pp.launches[q],
+                 "bytes": pp.bytes_per_launch[q]} for q in range(pp.count)]
 
     def close(self):
         if getattr(self, "_h", None):

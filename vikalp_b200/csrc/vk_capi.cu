@@ -171,6 +171,16 @@ int vk_pdhg_set_options(vk_pdhg *h, const vk_options *opts) {
     });
 }
 
+int vk_pdhg_profile(vk_pdhg *h, int64_t iterations, vk_pass_profile *out) {
+    return guarded([&] {
+        if (!h || !out) return set_error(VK_ERR_INVALID, "null argument");
+        if (iterations < 1 || iterations > 100000) return set_error(VK_ERR_INVALID, "iterations must be in [1, 100000]");
+        if (!h->solver->profile(iterations, out))
+            return set_error(VK_ERR_UNSUPPORTED, "this scheme has no profiling path (VK_ALGO_REFERENCE has)");
+        return VK_OK;
+    });
+}
+
 void vk_pdhg_destroy(vk_pdhg *h) {
     try {
         delete h;

@@ -3,6 +3,7 @@
 #include "vk_csr.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -84,6 +85,20 @@ __global__ void gather_values_kernel(const int *__restrict__ perm, const TS *__r
         dst[t] = static_cast<TD>(src[perm[t]]);
 }
 
+// chunks[c] = first row r with cost(r) >= c * kChunkCost, cost(r) = ro[r] +
+// kRowCost * r (monotone); chunks[nchunks] = rows. Thread per r in [0, rows].
+__global__ void chunk_rows_kernel(const int *__restrict__ ro, int rows, int nchunks, int *__restrict__ chunks) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r > rows) return;
+    const int64_t hi = static_cast<int64_t>(ro[r]) + static_cast<int64_t>(kRowCost) * r;
+    const int64_t lo = r == 0 ? -1 : static_cast<int64_t>(ro[r - 1]) + static_cast<int64_t>(kRowCost) * (r - 1);
+    // chunk boundaries c * K in (lo, hi]
+    int64_t c0 = lo < 0 ? 0 : lo / kChunkCost + 1;
+    const int64_t c1 = hi / kChunkCost;
+    for (int64_t c = c0; c <= c1 && c < nchunks; ++c) chunks[c] = r;
+    if (r == rows) chunks[nchunks] = rows;
+}
+
 int grid_for(int64_t n, int threads = 256) {
     const int64_t b = (n + threads - 1) / threads;
     return static_cast<int>(b < 148 * 32 ? (b > 0 ? b : 1) : 148 * 32);
@@ -144,6 +159,15 @@ void build_tiles(CsrPattern32 &p, cudaStream_t s, const unsigned char *breaks) {
     VK_LAUNCH_CHECK();
     p.tile_k.reset(count);
     tile_k_kernel<<<ceil_div(count, 256), 256, 0, s>>>(p.ro.get(), p.tiles.get(), count, p.tile_k.get());
+    VK_LAUNCH_CHECK();
+    // cost-balanced row ranges for the hybrid kernel
+    int nnz_total = 0;
+    VK_CUDA(cudaMemcpyAsync(&nnz_total, p.ro.get() + rows, sizeof(int), cudaMemcpyDeviceToHost, s));
+    VK_CUDA(cudaStreamSynchronize(s));
+    const int64_t cost = static_cast<int64_t>(nnz_total) + static_cast<int64_t>(kRowCost) * rows;
+    p.nchunks = rows > 0 ? static_cast<int>((cost - 1) / kChunkCost + 1) : 0;
+    p.chunks.reset(p.nchunks + 1);
+    chunk_rows_kernel<<<ceil_div(rows + 1, 256), 256, 0, s>>>(p.ro.get(), rows, p.nchunks, p.chunks.get());
     VK_LAUNCH_CHECK();
     VK_CUDA(cudaStreamSynchronize(s));
 }
@@ -265,9 +289,20 @@ __global__ void fill_kernel(T *a, int64_t n, T v) {
 }
 } // namespace
 
+int forced_variant() {
+    const char *e = std::getenv("VIKALP_B200_VARIANT");
+    if (!e || !*e) return -1;
+    const int v = std::atoi(e);
+    return v >= 0 && v < kFastVariants ? v : -1;
+}
+
 template <class T>
 void autotune_pattern(CsrPattern32 &p, const T *val, cudaStream_t s, int64_t min_nnz) {
     p.variant = 0;
+    if (const int f = forced_variant(); f >= 0) {
+        p.variant = f;
+        return;
+    }
     if (p.nnz < min_nnz || p.rows == 0 || p.cols == 0) return;
     DevBuf<T> x(p.cols), y(p.rows);
     fill_kernel<T><<<grid_for(p.cols), 256, 0, s>>>(x.get(), p.cols, T(1));

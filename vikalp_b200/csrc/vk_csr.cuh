@@ -53,7 +53,8 @@ struct CsrPattern32 {
     int rows = 0, cols = 0;
     int64_t nnz = 0;
     DevBuf<int> ro, ci, tiles, tile_k;
-    int ntiles = 0;
+    DevBuf<int> chunks; // cost-balanced row ranges for the hybrid kernel (nchunks+1 row starts)
+    int ntiles = 0, nchunks = 0;
     int max_row = 0;
     int variant = 0; // FAST kernel variant picked by autotune_pattern
 };
@@ -71,15 +72,16 @@ struct CsrView {
     const T *__restrict__ val;
     const int *__restrict__ tiles;
     const int *__restrict__ tile_k;
+    const int *__restrict__ chunks;
     int *err;
-    int rows, cols, ntiles;
+    int rows, cols, ntiles, nchunks;
     int variant; // FAST kernel variant (autotuned per matrix)
 };
 
 template <class T>
 inline CsrView<T> view(const CsrPattern32 &p, const T *val) {
-    return CsrView<T>{p.ro.get(), p.ci.get(), val, p.tiles.get(), p.tile_k.get(), device_error_flag(),
-                      p.rows, p.cols, p.ntiles, p.variant};
+    return CsrView<T>{p.ro.get(), p.ci.get(), val, p.tiles.get(), p.tile_k.get(), p.chunks.get(), device_error_flag(),
+                      p.rows, p.cols, p.ntiles, p.nchunks, p.variant};
 }
 
 // Rounded multiply / add that the compiler never contracts into an FMA, so the
@@ -116,19 +118,25 @@ struct Gathers {
 //   PIPE  prefetch the next batch's indices / values while the current batch
 //         gathers and reduces (SUB = 0 only)
 //   MINB  resident CTAs per SM the register allocation is held to
+//   HYB   > 0: the hybrid kernel (tile_kernel_hyb): a lane sums its own row
+//         when it has at most HYB nonzeros, longer rows are shared by
+//         sub-warps of SUB lanes (or by the whole warp)
 struct FastVariant {
-    int u, pipe, minb, sub;
+    int u, pipe, minb, sub, hyb;
 };
-constexpr int kFastVariants = 8;
+constexpr int kFastVariants = 11;
 __host__ __device__ constexpr FastVariant fast_variant(int v) {
-    return v == 0   ? FastVariant{4, 1, 12, 0}
-           : v == 1 ? FastVariant{8, 1, 8, 0}
-           : v == 2 ? FastVariant{8, 0, 12, 0}
-           : v == 3 ? FastVariant{16, 0, 8, 0}
-           : v == 4 ? FastVariant{2, 1, 16, 0}
-           : v == 5 ? FastVariant{2, 0, 12, 8}
-           : v == 6 ? FastVariant{4, 0, 12, 4}
-                    : FastVariant{2, 0, 12, 16};
+    return v == 0   ? FastVariant{4, 1, 12, 0, 0}
+           : v == 1 ? FastVariant{8, 1, 8, 0, 0}
+           : v == 2 ? FastVariant{8, 0, 12, 0, 0}
+           : v == 3 ? FastVariant{16, 0, 8, 0, 0}
+           : v == 4 ? FastVariant{2, 1, 16, 0, 0}
+           : v == 5 ? FastVariant{2, 0, 12, 8, 0}
+           : v == 6 ? FastVariant{4, 0, 12, 4, 0}
+           : v == 7 ? FastVariant{2, 0, 12, 16, 0}
+           : v == 8 ? FastVariant{4, 0, 8, 8, 4}
+           : v == 9 ? FastVariant{2, 0, 12, 8, 2}
+                    : FastVariant{2, 0, 12, 4, 4};
 }
 
 template <class T, class A, int NV, class Epi, int U, bool PIPE, int MINB>
@@ -469,6 +477,180 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     epi.finish(red, scratch, blockIdx.x);
 }
 
+// Hybrid variant. Rows go in groups of 32, one per lane; every lane loads its
+// row's bounds and epilogue inputs first. A lane with at most S nonzeros sums
+// its own row (S loads in flight, left to right). The group's longer rows are
+// then taken, in order, by the whole warp one at a time when a row is long
+// (more than 4*L*U nonzeros), else 32/L at a time by sub-warps of L lanes
+// (U loads per lane in flight, L-wide shuffle reduction); each sum goes back
+// to the row's own lane by a shuffle, and every lane runs its row's epilogue,
+// so the epilogue's loads and stores are coalesced across the group.
+// Work: cost-balanced row ranges (chunks, about kChunkCost nonzeros-plus-4-
+// per-row each) round robin over the persistent grid, or the tile schedule's
+// tiles when the epilogue reduces per tile or skips tiles.
+constexpr int kChunkCost = 1024;
+constexpr int kRowCost = 4;
+
+template <class T, class A, int NV, class Epi, int S, int L, int U, int MINB>
+__global__ void __launch_bounds__(kTileThreads, MINB)
+    tile_kernel_hyb(CsrView<T> M, Gathers<T, NV> g, Epi epi) {
+    static_assert(L == 2 || L == 4 || L == 8 || L == 16, "sub-warp width");
+    if (epi.skip()) return;
+    constexpr int NR = Epi::NR;
+    constexpr int G = 32 / L;
+    constexpr int kWarpRow = 4 * L * U; // longer rows take the whole warp
+    using Pre = typename Epi::Pre;
+    __shared__ double scratch[32 * 8];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int sl = lane % L, sw = lane / L;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    double red[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) red[r] = 0.0;
+    A gs[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) gs[q] = epi.gscale(q);
+
+    // rows [rb, re), re - rb <= 32
+    auto group = [&](int rb, int re) {
+        const int r = rb + lane;
+        const bool valid = r < re;
+        int a = 0, b = 0;
+        if (valid) {
+            a = __ldg(M.ro + r);
+            b = __ldg(M.ro + r + 1);
+        }
+        Pre pre{};
+        if (valid) pre = epi.load(r);
+        const int len = b - a;
+        A sum[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) sum[q] = A(0);
+        if (valid && len <= S) {
+            int c[S];
+            T v[S];
+#pragma unroll
+            for (int u = 0; u < S; ++u) {
+                c[u] = u < len ? __ldg(M.ci + a + u) : 0;
+                v[u] = u < len ? __ldg(M.val + a + u) : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < S; ++u)
+                if (u < len) {
+#pragma unroll
+                    for (int q = 0; q < NV; ++q)
+                        sum[q] += static_cast<A>(v[u]) * (gs[q] * static_cast<A>(__ldg(g.p[q] + c[u])));
+                }
+        }
+        unsigned lm = __ballot_sync(FULL, valid && len > S);
+        while (lm) {
+            const int first = __ffs(lm) - 1;
+            const int fa = __shfl_sync(FULL, a, first), fb = __shfl_sync(FULL, b, first);
+            if (fb - fa > kWarpRow) {
+                // one long row, the whole warp
+                A part[NV];
+#pragma unroll
+                for (int q = 0; q < NV; ++q) part[q] = A(0);
+                for (int kb = fa; kb < fb; kb += 32 * U) {
+                    int c[U];
+                    T v[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int k = kb + 32 * u + lane;
+                        c[u] = k < fb ? __ldg(M.ci + k) : 0;
+                        v[u] = k < fb ? __ldg(M.val + k) : T(0);
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+                        if (kb + 32 * u + lane < fb) {
+#pragma unroll
+                            for (int q = 0; q < NV; ++q)
+                                part[q] += static_cast<A>(v[u]) * (gs[q] * static_cast<A>(__ldg(g.p[q] + c[u])));
+                        }
+                }
+#pragma unroll
+                for (int q = 0; q < NV; ++q) {
+                    const A t = warp_sum(part[q]);
+                    if (lane == first) sum[q] = t;
+                }
+                lm &= lm - 1u;
+                continue;
+            }
+            // up to G rows, one per sub-warp: sub-warp w takes the (w+1)-th set bit
+            const unsigned pos = __fns(lm, 0, sw + 1);
+            const bool has = pos < 32u;
+            const int src = has ? static_cast<int>(pos) : 0;
+            const int ra = __shfl_sync(FULL, a, src), rz = __shfl_sync(FULL, b, src);
+            A part[NV];
+#pragma unroll
+            for (int q = 0; q < NV; ++q) part[q] = A(0);
+            if (has) {
+                for (int kb = ra + sl; kb < rz; kb += U * L) {
+                    int c[U];
+                    T v[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int k = kb + u * L;
+                        c[u] = k < rz ? __ldg(M.ci + k) : 0;
+                        v[u] = k < rz ? __ldg(M.val + k) : T(0);
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+                        if (kb + u * L < rz) {
+#pragma unroll
+                            for (int q = 0; q < NV; ++q)
+                                part[q] += static_cast<A>(v[u]) * (gs[q] * static_cast<A>(__ldg(g.p[q] + c[u])));
+                        }
+                }
+            }
+#pragma unroll
+            for (int o = L / 2; o > 0; o >>= 1)
+#pragma unroll
+                for (int q = 0; q < NV; ++q) part[q] += __shfl_xor_sync(FULL, part[q], o, L);
+            // back to the owners: the lane of the k-th set bit (k < G) reads sub-warp k's lane 0
+            const int rank = __popc(lm & lt_mask);
+            const bool mine = ((lm >> lane) & 1u) && rank < G;
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                const A t = __shfl_sync(FULL, part[q], mine ? rank * L : 0);
+                if (mine) sum[q] = t;
+            }
+#pragma unroll
+            for (int i = 0; i < G; ++i) lm &= lm - 1u;
+        }
+        if (valid) {
+            A s2[NV];
+#pragma unroll
+            for (int q = 0; q < NV; ++q) s2[q] = epi.init(r, q) + sum[q];
+            epi.row_pre(r, s2, pre, red);
+        }
+    };
+
+    const int W = gridDim.x * kWarps;
+    const int wid = blockIdx.x * kWarps + warp;
+    if constexpr (Epi::kPerTile || Epi::kSkipTiles) {
+        for (int tile = wid; tile < M.ntiles; tile += W) {
+            if (epi.skip_tile(tile)) continue;
+            const int r0 = __ldg(M.tiles + tile), r1 = __ldg(M.tiles + tile + 1);
+            for (int rb = r0; rb < r1; rb += 32) group(rb, rb + 32 < r1 ? rb + 32 : r1);
+            if constexpr (Epi::kPerTile) {
+#pragma unroll
+                for (int r = 0; r < NR; ++r) red[r] = warp_sum(red[r]);
+                if (lane == 0) epi.tile_done(tile, red);
+#pragma unroll
+                for (int r = 0; r < NR; ++r) red[r] = 0.0;
+            }
+        }
+    } else {
+        for (int ch = wid; ch < M.nchunks; ch += W) {
+            const int r0 = __ldg(M.chunks + ch), r1 = __ldg(M.chunks + ch + 1);
+            for (int rb = r0; rb < r1; rb += 32) group(rb, rb + 32 < r1 ? rb + 32 : r1);
+        }
+    }
+    epi.finish(red, scratch, blockIdx.x);
+}
+
 // Parity kernel: one thread per row, the reference's left-to-right order.
 template <class T, class A, int NV, class Epi>
 __global__ void __launch_bounds__(kTileThreads)
@@ -514,7 +696,9 @@ template <class T, class A, int NV, class Epi, int V>
 inline int launch_fast(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi &epi, cudaStream_t s) {
     constexpr FastVariant fv = fast_variant(V);
     void (*kernel)(CsrView<T>, Gathers<T, NV>, Epi);
-    if constexpr (fv.sub > 0)
+    if constexpr (fv.hyb > 0)
+        kernel = tile_kernel_hyb<T, A, NV, Epi, fv.hyb, fv.sub, fv.u, fv.minb>;
+    else if constexpr (fv.sub > 0)
         kernel = tile_kernel_sub<T, A, NV, Epi, (fv.sub > 0 ? fv.sub : 32), fv.u, fv.minb>;
     else
         kernel = tile_kernel_fast<T, A, NV, Epi, fv.u, fv.pipe != 0, fv.minb>;
@@ -549,6 +733,9 @@ inline int launch_tiles(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi 
     case 5: return launch_fast<T, A, NV, Epi, 5>(M, g, epi, s);
     case 6: return launch_fast<T, A, NV, Epi, 6>(M, g, epi, s);
     case 7: return launch_fast<T, A, NV, Epi, 7>(M, g, epi, s);
+    case 8: return launch_fast<T, A, NV, Epi, 8>(M, g, epi, s);
+    case 9: return launch_fast<T, A, NV, Epi, 9>(M, g, epi, s);
+    case 10: return launch_fast<T, A, NV, Epi, 10>(M, g, epi, s);
     default: return launch_fast<T, A, NV, Epi, 0>(M, g, epi, s);
     }
 }
@@ -608,7 +795,12 @@ void expand_rows(const CsrPattern32 &p, int *rowidx, cudaStream_t s);
 // Autotuner: times every FAST kernel variant on this matrix (a plain product
 // into scratch vectors, a few launches each) and stores the fastest in
 // p.variant. Matrices below `min_nnz` keep variant 0.
+// The environment variable VIKALP_B200_VARIANT=<v> (0 <= v < kFastVariants)
+// pins every pattern (and every tuned pass) to variant v instead, at any size:
+// a knob for tests that run whole solves on each kernel variant.
 template <class T>
 void autotune_pattern(CsrPattern32 &p, const T *val, cudaStream_t s, int64_t min_nnz = 200000);
+// The pinned variant, or -1.
+int forced_variant();
 
 } // namespace vk

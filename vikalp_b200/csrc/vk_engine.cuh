@@ -14,6 +14,16 @@ struct RunInfo {
     double iterate_seconds = 0.0;
 };
 
+// Device time per kernel kind of the iteration loop (vk_pdhg_profile).
+struct PassProfile {
+    static constexpr int kMax = 8;
+    int count = 0;
+    const char *name[kMax] = {};
+    double ms[kMax] = {};         // summed device time (CUDA events)
+    long long launches[kMax] = {};
+    double bytes[kMax] = {};      // algorithmic bytes per launch (0: not modelled)
+};
+
 class Engine {
 public:
     virtual ~Engine() = default;
@@ -24,6 +34,10 @@ public:
                      RunInfo &info, std::chrono::steady_clock::time_point started) = 0;
     // Per-solve limits and tolerances (the structural options never change).
     virtual void set_limits(const vk_options &o) = 0;
+    // Runs `iterations` iterations from a cold start with the model's bounds,
+    // launched one by one (no graph) with CUDA events around each kernel kind
+    // on the engine's stream. False when the engine has no profiling path.
+    virtual bool profile(long long, PassProfile &) { return false; }
 };
 
 std::unique_ptr<Engine> make_reference_engine(const DeviceModel &dm, const vk_options &o, cudaStream_t s);

@@ -181,6 +181,7 @@ std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s) {
         dm->h_qro.assign(p.Q.row_offsets, p.Q.row_offsets + n + 1);
         dm->h_qci.assign(p.Q.col_indices, p.Q.col_indices + dm->q_nnz);
         dm->h_qv.assign(p.Q.values, p.Q.values + dm->q_nnz);
+        autotune_pattern<double>(dm->q, dm->q_val.get(), s);
     }
     auto up = [&](DevBuf<double> &b, const double *h, int64_t k) {
         b.reset(k > 0 ? k : 1);
@@ -384,6 +385,21 @@ std::string Solver::set_options(const vk_options &o) {
     opts_ = o;
     engine_->set_limits(o);
     return "";
+}
+
+bool Solver::profile(long long iterations, vk_pass_profile *out) {
+    VK_CUDA(cudaSetDevice(opts_.device));
+    PassProfile pp;
+    if (!engine_->profile(iterations, pp)) return false;
+    *out = vk_pass_profile{};
+    out->count = pp.count;
+    for (int q = 0; q < pp.count && q < 8; ++q) {
+        std::snprintf(out->name[q], sizeof(out->name[q]), "%s", pp.name[q] ? pp.name[q] : "");
+        out->launches[q] = pp.launches[q];
+        out->ms_per_launch[q] = pp.launches[q] ? pp.ms[q] / static_cast<double>(pp.launches[q]) : 0.0;
+        out->bytes_per_launch[q] = pp.bytes[q];
+    }
+    return true;
 }
 
 Solver::~Solver() {

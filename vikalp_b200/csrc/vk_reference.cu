@@ -17,12 +17,24 @@
 // Every floating-point operation keeps the reference's operands and order,
 // with no FMA contraction; with VK_SPMV_SEQUENTIAL the sparse sums are the
 // reference's left-to-right sums too, so iterates match it bit for bit.
+//
+// With the FAST product order (sums in warp order, so iterates agree with the
+// reference to rounding only) the iteration drops two of its passes' work:
+//   * K xbar = 2 K x_{k+1} - K x_k by linearity (pdhg.cpp:102-105 against
+//     116): the row pass gathers x_{k+1} only and keeps K x_{k+1} for the next
+//     iteration (kx), so each nonzero is gathered once per pass;
+//   * the primal step is done in the column pass's epilogue on the iterations
+//     whose control step cannot change tau or the restart flag (all but the
+//     every-50th, pdhg.cpp:133), so the separate primal kernel runs once per
+//     50 iterations.
 // Chunks of iterations are captured in a CUDA graph; the host only polls a
 // done flag between chunks.
 #include "vk_engine.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <limits>
+#include <vector>
 
 namespace vk {
 namespace {
@@ -154,6 +166,85 @@ struct RefRowEpi : EpiBase<double> {
     }
 };
 
+// True when the control step of iteration k (which judges the metric of
+// iteration k-1) may change tau / sigma or set the restart flag: pdhg.cpp:133,
+// every 50 iterations after the first.
+__device__ __forceinline__ bool ref_policy_iter(long long k) { return k >= 51 && (k - 1) % 50 == 0; }
+
+// FAST column pass: the stationarity norm of iteration k-1 as RefColEpi, and
+// the primal step of iteration k (ref_primal_kernel's arithmetic) in the same
+// epilogue unless the control step may still change tau; then K'y goes to aty
+// for the separate primal kernel.
+template <bool QP>
+struct RefColFastEpi : EpiBase<double> {
+    RefCtl *ctl;
+    double *aty, *xn;
+    const double *x, *c, *l, *u, *qx;
+    struct Pre {
+        double x, c, l, u, qx;
+    };
+    __device__ bool skip() const { return ctl->done != 0; }
+    __device__ Pre load(int j) const { return Pre{x[j], c[j], l[j], u[j], QP ? qx[j] : 0.0}; }
+    __device__ void row_pre(int j, const double (&s)[1], const Pre &p, double (&red)[1]) const {
+        const long long k = __ldg(&ctl->iter);
+        const double g = QP ? __dadd_rn(s[0], __dadd_rn(p.c, p.qx)) : __dadd_rn(s[0], p.c);
+        if (k >= 1) {
+            const double px = clampbox(__dadd_rn(-g, p.x), p.l, p.u);
+            red[0] = smax(red[0], fabs(__dadd_rn(-px, p.x)));
+        }
+        if (ref_policy_iter(k)) {
+            aty[j] = s[0];
+            return;
+        }
+        const double tau = __ldg(&ctl->tau);
+        double v;
+        if (QP) {
+            v = __dadd_rn(__dmul_rn(-tau, g), p.x);
+        } else {
+            const double t = __dadd_rn(__dmul_rn(-tau, p.c), p.x);
+            v = __dadd_rn(__dmul_rn(-tau, s[0]), t);
+        }
+        xn[j] = clampbox(v, p.l, p.u);
+    }
+    __device__ void finish(double (&red)[1], double *scratch, int) const {
+        const double v = block_max_nonneg(red[0], scratch);
+        if (threadIdx.x == 0) atomic_max_nonneg(&ctl->rd, v);
+    }
+};
+
+// FAST row pass: gathers x_{k+1} once; K xbar = K x_{k+1} after a restart,
+// else 2 K x_{k+1} - K x_k (the extrapolation of pdhg.cpp:102-104 applied to
+// the products); then RefRowEpi's dual step and primal norm. kx[i] holds
+// K x_k on entry and K x_{k+1} on exit.
+struct RefRowFastEpi : EpiBase<double> {
+    RefCtl *ctl;
+    double *y, *kx;
+    const double *rl, *ru;
+    struct Pre {
+        double y, rl, ru, kx;
+    };
+    __device__ bool skip() const { return ctl->done != 0; }
+    __device__ Pre load(int i) const { return Pre{y[i], rl[i], ru[i], kx[i]}; }
+    __device__ void row_pre(int i, const double (&s)[1], const Pre &p, double (&red)[1]) const {
+        const double sigma = ctl->sigma, inv = ctl->inv_sigma;
+        const double kxn = s[0];
+        const double kxbar = ctl->restart ? kxn : __dadd_rn(__dmul_rn(2.0, kxn), -p.kx);
+        kx[i] = kxn;
+        const double yarg = __dadd_rn(__dmul_rn(sigma, kxbar), p.y);
+        const double yp = clampbox(__dmul_rn(inv, yarg), p.rl, p.ru);
+        y[i] = __dadd_rn(__dmul_rn(-sigma, yp), yarg);
+        const double pax = clampbox(kxn, p.rl, p.ru);
+        red[0] = smax(red[0], fabs(__dadd_rn(pax, -kxn)));
+    }
+    __device__ void finish(double (&red)[1], double *scratch, int block) const {
+        const double v = block_max_nonneg(red[0], scratch);
+        if (threadIdx.x == 0) {
+            atomic_max_nonneg(&ctl->rp, v);
+            if (block == 0) atomicAdd(reinterpret_cast<unsigned long long *>(&ctl->iter), 1ull);
+        }
+    }
+};
+
 struct StoreEpi : EpiRow<double, StoreEpi> {
     RefCtl *ctl;
     double *out;
@@ -200,13 +291,17 @@ __global__ void ref_control_kernel(RefCtl *ctl) {
     *ctl = c;
 }
 
+// xbar may be null (FAST order: the row pass extrapolates the products
+// instead); policy_only: only on the iterations whose primal step the FAST
+// column pass left undone.
 template <bool QP>
 __global__ void ref_primal_kernel(const RefCtl *__restrict__ ctl, const double *__restrict__ x,
                                   const double *__restrict__ aty, const double *__restrict__ c,
                                   const double *__restrict__ qx, const double *__restrict__ l,
                                   const double *__restrict__ u, int n, double *__restrict__ xn,
-                                  double *__restrict__ xbar) {
+                                  double *__restrict__ xbar, bool policy_only) {
     if (ctl->done) return;
+    if (policy_only && !ref_policy_iter(ctl->iter)) return;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const double tau = ctl->tau;
@@ -221,7 +316,7 @@ __global__ void ref_primal_kernel(const RefCtl *__restrict__ ctl, const double *
     }
     v = clampbox(v, l[j], u[j]);
     xn[j] = v;
-    xbar[j] = ctl->restart ? v : __dadd_rn(__dmul_rn(2.0, v), -xj);
+    if (xbar) xbar[j] = ctl->restart ? v : __dadd_rn(__dmul_rn(2.0, v), -xj);
 }
 
 class ReferenceEngine final : public Engine {
@@ -277,8 +372,9 @@ public:
         // Iterates.
         x_[0].reset(n);
         x_[1].reset(n);
-        xbar_.reset(n);
+        if (exact_) xbar_.reset(n);
         aty_.reset(n);
+        if (!exact_) kx_.reset(m > 0 ? m : 1);
         y_.reset(m > 0 ? m : 1);
         qx_.reset(dm.qp ? n : 1);
         sl_.reset(n);
@@ -286,33 +382,88 @@ public:
         ctl_.reset(1);
         hctl_.reset(1);
         // Iterations per graph chunk: enough to amortise the poll, few enough
-        // to stop promptly.
+        // to stop promptly. FAST order: a multiple of the 50-iteration step
+        // rule period, so every graph starts at an iteration k = 0 (mod 50)
+        // and only its second iteration (k = 1 mod 50) can need the separate
+        // primal kernel.
         const int64_t work = dm.nnz + dm.m + dm.n;
-        chunk_ = work < (1 << 20) ? 64 : (work < (1 << 24) ? 16 : 4);
+        graph_iters_ = work < (1 << 20) ? 128 : (work < (1 << 24) ? 32 : 8);
+        if (!exact_) graph_iters_ = work < (1 << 20) ? 150 : 50;
+        tune_passes();
     }
 
     ~ReferenceEngine() override {
         if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     }
 
-    void run(const double *d_warm, const double *d_lo, const double *d_hi, double *d_xo, double *d_yo,
-             RunInfo &info, std::chrono::steady_clock::time_point started) override {
+    // Starting point and control block of a solve (pdhg.cpp:61-80).
+    void prepare(const double *d_warm, const double *d_lo, const double *d_hi, long long limit, double tol) {
         const int m = dm_.m, n = dm_.n;
         ref_prepare_kernel<<<grid1d(n), 256, 0, s_>>>(d_warm, d_lo, d_hi, cs_.get(), n, sl_.get(), su_.get(),
                                                       x_[0].get());
         VK_LAUNCH_CHECK();
         if (m > 0) VK_CUDA(cudaMemsetAsync(y_.get(), 0, m * sizeof(double), s_));
         if (dm_.qp) q_product(x_[0].get(), nullptr);
+        if (!exact_ && m > 0) {
+            // kx = K x_0 for the first extrapolated product.
+            StoreEpi e;
+            e.ctl = nullptr;
+            e.out = kx_.get();
+            tiles(view(dm_.a, ka_.get()), Gathers<double, 1>{{x_[0].get()}}, e);
+        }
         RefCtl c{};
         c.tau = c.sigma = max_step_;
         c.inv_sigma = 1.0 / c.sigma;
         c.max_step = max_step_;
         c.previous = std::numeric_limits<double>::infinity();
         c.last_metric = std::numeric_limits<double>::quiet_NaN();
-        c.tol = smax(o_.primal_tolerance, o_.dual_tolerance);
-        c.limit = o_.iteration_limit;
+        c.tol = tol;
+        c.limit = limit;
         c.status = VK_STATUS_NOT_SOLVED;
         VK_CUDA(cudaMemcpyAsync(ctl_.get(), &c, sizeof(c), cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaStreamSynchronize(s_)); // c lives on this stack frame
+    }
+
+    bool profile(long long iterations, PassProfile &pp) override {
+        const int m = dm_.m, n = dm_.n;
+        prepare(nullptr, dm_.vl.get(), dm_.vu.get(), iterations, 0.0);
+        const int kinds = 3;
+        std::vector<cudaEvent_t> ev(static_cast<size_t>(iterations) * (kinds + 1));
+        for (auto &e : ev) VK_CUDA(cudaEventCreate(&e));
+        for (long long k = 0; k < iterations; ++k)
+            iteration_parts(static_cast<int>(k % (2 * 50)), &ev[static_cast<size_t>(k) * (kinds + 1)]);
+        VK_CUDA(cudaStreamSynchronize(s_));
+        check_device_error(s_);
+        pp = PassProfile{};
+        pp.count = kinds;
+        pp.name[0] = "column pass (K'y, primal step)";
+        pp.name[1] = "control + primal kernel";
+        pp.name[2] = dm_.qp ? "Q pass + row pass" : "row pass (K x, dual step)";
+        const double s = 8.0; // float64 values and vectors
+        const double nnz = static_cast<double>(dm_.nnz);
+        // Algorithmic bytes: values + int32 indices, int32 offsets, the
+        // gathered vector once, the per-row / per-column vectors of the
+        // epilogue (see the epilogues above).
+        pp.bytes[0] = nnz * (s + 4) + 4.0 * (n + 1) + s * m + s * n * (dm_.qp ? 6 : 5);
+        pp.bytes[1] = 0.0;
+        pp.bytes[2] = nnz * (s + 4) + 4.0 * (m + 1) + s * n + s * m * (exact_ ? 4 : 6) + (exact_ ? s * n : 0.0);
+        for (long long k = 0; k < iterations; ++k) {
+            for (int q = 0; q < kinds; ++q) {
+                float ms = 0.f;
+                VK_CUDA(cudaEventElapsedTime(&ms, ev[static_cast<size_t>(k) * (kinds + 1) + q],
+                                             ev[static_cast<size_t>(k) * (kinds + 1) + q + 1]));
+                pp.ms[q] += ms;
+                pp.launches[q] += 1;
+            }
+        }
+        for (auto &e : ev) cudaEventDestroy(e);
+        return true;
+    }
+
+    void run(const double *d_warm, const double *d_lo, const double *d_hi, double *d_xo, double *d_yo,
+             RunInfo &info, std::chrono::steady_clock::time_point started) override {
+        const int m = dm_.m, n = dm_.n;
+        prepare(d_warm, d_lo, d_hi, o_.iteration_limit, smax(o_.primal_tolerance, o_.dual_tolerance));
         if (!graph_exec_) capture();
         cudaEvent_t e0, e1;
         VK_CUDA(cudaEventCreate(&e0));
@@ -368,7 +519,21 @@ private:
         tiles(view(dm_.q, kq_.get()), Gathers<double, 1>{{x}}, e);
     }
 
-    void iteration(int k) {
+    void iteration(int k) { iteration_parts(k, nullptr); }
+
+    // One iteration; k is its position in a graph (or a profiling run) whose
+    // first iteration is k = 0 (mod 50) globally. ev: null, or 4 events
+    // recorded before the column pass, after it, before the row pass and
+    // after it.
+    void iteration_parts(int k, cudaEvent_t *ev) {
+        auto mark = [&](int q) {
+            if (ev) VK_CUDA(cudaEventRecord(ev[q], s_));
+        };
+        mark(0);
+        if (!exact_) {
+            iteration_fast(k, mark);
+            return;
+        }
         const int n = dm_.n;
         double *cur = x_[k % 2].get(), *nxt = x_[(k + 1) % 2].get();
         if (dm_.qp) {
@@ -380,15 +545,17 @@ private:
             fill_col(e, cur);
             tiles(view(dm_.at, kat_.get()), Gathers<double, 1>{{y_.get()}}, e);
         }
+        mark(1);
         ref_control_kernel<<<1, 1, 0, s_>>>(ctl_.get());
         VK_LAUNCH_CHECK();
         if (dm_.qp)
             ref_primal_kernel<true><<<grid1d(n), 256, 0, s_>>>(ctl_.get(), cur, aty_.get(), sc_.get(), qx_.get(),
-                                                               sl_.get(), su_.get(), n, nxt, xbar_.get());
+                                                               sl_.get(), su_.get(), n, nxt, xbar_.get(), false);
         else
             ref_primal_kernel<false><<<grid1d(n), 256, 0, s_>>>(ctl_.get(), cur, aty_.get(), sc_.get(), nullptr,
-                                                                sl_.get(), su_.get(), n, nxt, xbar_.get());
+                                                                sl_.get(), su_.get(), n, nxt, xbar_.get(), false);
         VK_LAUNCH_CHECK();
+        mark(2);
         if (dm_.qp) q_product(nxt, ctl_.get());
         RefRowEpi r;
         r.ctl = ctl_.get();
@@ -401,6 +568,53 @@ private:
             // No rows: the iteration still completes.
             bump_iter_kernel_launch();
         }
+        mark(3);
+    }
+
+    // FAST order; k is the position in the graph, whose first iteration is
+    // k = 0 (mod 50) globally.
+    template <class Mark>
+    void iteration_fast(int k, Mark &mark) {
+        const int n = dm_.n;
+        double *cur = x_[k % 2].get(), *nxt = x_[(k + 1) % 2].get();
+        if (dm_.qp) {
+            RefColFastEpi<true> e;
+            fill_col(e, cur);
+            e.xn = nxt;
+            tiles(col_view(), Gathers<double, 1>{{y_.get()}}, e);
+        } else {
+            RefColFastEpi<false> e;
+            fill_col(e, cur);
+            e.xn = nxt;
+            tiles(col_view(), Gathers<double, 1>{{y_.get()}}, e);
+        }
+        mark(1);
+        ref_control_kernel<<<1, 1, 0, s_>>>(ctl_.get());
+        VK_LAUNCH_CHECK();
+        if (k % 50 == 1) {
+            if (dm_.qp)
+                ref_primal_kernel<true><<<grid1d(n), 256, 0, s_>>>(ctl_.get(), cur, aty_.get(), sc_.get(),
+                                                                   qx_.get(), sl_.get(), su_.get(), n, nxt, nullptr,
+                                                                   true);
+            else
+                ref_primal_kernel<false><<<grid1d(n), 256, 0, s_>>>(ctl_.get(), cur, aty_.get(), sc_.get(), nullptr,
+                                                                    sl_.get(), su_.get(), n, nxt, nullptr, true);
+            VK_LAUNCH_CHECK();
+        }
+        mark(2);
+        if (dm_.qp) q_product(nxt, ctl_.get());
+        if (dm_.m > 0) {
+            RefRowFastEpi r;
+            r.ctl = ctl_.get();
+            r.y = y_.get();
+            r.kx = kx_.get();
+            r.rl = srl_.get();
+            r.ru = sru_.get();
+            tiles(row_view(), Gathers<double, 1>{{nxt}}, r);
+        } else {
+            bump_iter_kernel_launch();
+        }
+        mark(3);
     }
 
     template <class E>
@@ -416,9 +630,92 @@ private:
 
     void bump_iter_kernel_launch();
 
+    // The two fused passes with the kernel variant tuned for their epilogue.
+    CsrView<double> col_view() const {
+        CsrView<double> v = view(dm_.at, kat_.get());
+        if (col_variant_ >= 0) v.variant = col_variant_;
+        return v;
+    }
+    CsrView<double> row_view() const {
+        CsrView<double> v = view(dm_.a, ka_.get());
+        if (row_variant_ >= 0) v.variant = row_variant_;
+        return v;
+    }
+
+    // FAST order: times every kernel variant on the two fused passes
+    // themselves (their epilogues set the register pressure, so the plain
+    // product's choice need not carry over) from a prepared cold state, and
+    // keeps the fastest for each. The state is prepared again by every solve.
+    void tune_passes() {
+        if (const int f = forced_variant(); f >= 0) {
+            col_variant_ = row_variant_ = f;
+            return;
+        }
+        if (exact_ || dm_.nnz < 200000 || dm_.m == 0) return;
+        prepare(nullptr, dm_.vl.get(), dm_.vu.get(), std::numeric_limits<long long>::max() / 4, 0.0);
+        cudaEvent_t a, b;
+        VK_CUDA(cudaEventCreate(&a));
+        VK_CUDA(cudaEventCreate(&b));
+        auto time_it = [&](auto &&launch) {
+            launch();
+            float t[3];
+            for (float &x : t) {
+                VK_CUDA(cudaEventRecord(a, s_));
+                launch();
+                VK_CUDA(cudaEventRecord(b, s_));
+                VK_CUDA(cudaEventSynchronize(b));
+                VK_CUDA(cudaEventElapsedTime(&x, a, b));
+            }
+            std::sort(t, t + 3);
+            return t[1];
+        };
+        for (int pass = 0; pass < 2; ++pass) {
+            float best = 1e30f;
+            int best_v = 0;
+            for (int v = 0; v < kFastVariants; ++v) {
+                float ms;
+                if (pass == 0) {
+                    col_variant_ = v;
+                    ms = time_it([&] {
+                        if (dm_.qp) {
+                            RefColFastEpi<true> e;
+                            fill_col(e, x_[0].get());
+                            e.xn = x_[1].get();
+                            tiles(col_view(), Gathers<double, 1>{{y_.get()}}, e);
+                        } else {
+                            RefColFastEpi<false> e;
+                            fill_col(e, x_[0].get());
+                            e.xn = x_[1].get();
+                            tiles(col_view(), Gathers<double, 1>{{y_.get()}}, e);
+                        }
+                    });
+                } else {
+                    row_variant_ = v;
+                    ms = time_it([&] {
+                        RefRowFastEpi r;
+                        r.ctl = ctl_.get();
+                        r.y = y_.get();
+                        r.kx = kx_.get();
+                        r.rl = srl_.get();
+                        r.ru = sru_.get();
+                        tiles(row_view(), Gathers<double, 1>{{x_[1].get()}}, r);
+                    });
+                }
+                if (ms < best) {
+                    best = ms;
+                    best_v = v;
+                }
+            }
+            (pass == 0 ? col_variant_ : row_variant_) = best_v;
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        check_device_error(s_);
+    }
+
     void capture() {
         VK_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
-        for (int k = 0; k < 2 * chunk_; ++k) iteration(k);
+        for (int k = 0; k < graph_iters_; ++k) iteration(k);
         cudaGraph_t g;
         VK_CUDA(cudaStreamEndCapture(s_, &g));
         size_t nodes = 0;
@@ -433,11 +730,12 @@ private:
     cudaStream_t s_;
     bool exact_;
     DevBuf<double> rs_, cs_, ka_, kat_, kq_, sc_, srl_, sru_;
-    DevBuf<double> x_[2], xbar_, aty_, y_, qx_, sl_, su_;
+    DevBuf<double> x_[2], xbar_, aty_, y_, qx_, sl_, su_, kx_;
     DevBuf<RefCtl> ctl_;
     HostBuf<RefCtl> hctl_;
     double max_step_ = 0.0;
-    int chunk_ = 16;
+    int graph_iters_ = 32; // iterations per captured graph (even: x_ buffers alternate)
+    int col_variant_ = -1, row_variant_ = -1; // tuned kernel variants of the fused passes (-1: the pattern's)
     long long graph_nodes_ = 0;
     cudaGraphExec_t graph_exec_ = nullptr;
 };

@@ -51,6 +51,8 @@ public:
     void solve(const double *warm, const double *lo, const double *hi, vk_result *r);
     // Returns "" on success, else the reason the options were not accepted.
     std::string set_options(const vk_options &o);
+    // vk_pdhg_profile; false when the scheme has no profiling path.
+    bool profile(long long iterations, vk_pass_profile *out);
     const DeviceModel &model() const { return *dm_; }
     cudaStream_t stream() const { return stream_; }
 
