@@ -18,9 +18,11 @@ __global__ void narrow_kernel(const int64_t *__restrict__ src, int *__restrict__
         dst[i] = static_cast<int>(src[i]);
 }
 
-// flags[r] = 1 where a tile starts at row r (r == rows marks the end).
+// flags[r] = 1 where a tile starts at row r (r == rows marks the end): rows
+// longer than `short_max` alone, others grouped while their starts fall in
+// one `window`-sized window of the nonzero array, at most `rows_max` rows.
 __global__ void tile_flags_kernel(const int *__restrict__ ro, int rows, const unsigned char *__restrict__ breaks,
-                                  int *__restrict__ flags) {
+                                  int window, int short_max, int rows_max, int *__restrict__ flags) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r > rows) return;
     int f;
@@ -28,9 +30,9 @@ __global__ void tile_flags_kernel(const int *__restrict__ ro, int rows, const un
         f = 1;
     } else {
         const int a = ro[r - 1], b = ro[r], c = ro[r + 1];
-        const bool long_prev = (b - a) > kShortMax;
-        const bool long_here = (c - b) > kShortMax;
-        f = (long_prev || long_here || (a / kChunk) != (b / kChunk) || (r % kTileRows) == 0) ? 1 : 0;
+        const bool long_prev = (b - a) > short_max;
+        const bool long_here = (c - b) > short_max;
+        f = (long_prev || long_here || (a / window) != (b / window) || (r % rows_max) == 0) ? 1 : 0;
     }
     flags[r] = f;
 }
@@ -139,10 +141,14 @@ void check_device_error(cudaStream_t s) {
     }
 }
 
-void build_tiles(CsrPattern32 &p, cudaStream_t s, const unsigned char *breaks) {
+namespace {
+// One tile schedule: tiles[t] = first row, tile_k[t] = first nonzero.
+int schedule(const CsrPattern32 &p, cudaStream_t s, const unsigned char *breaks, int window, int short_max,
+             int rows_max, DevBuf<int> &tiles, DevBuf<int> &tile_k) {
     const int rows = p.rows;
     DevBuf<int> flags(rows + 1), idx(rows + 1);
-    tile_flags_kernel<<<ceil_div(rows + 1, 256), 256, 0, s>>>(p.ro.get(), rows, breaks, flags.get());
+    tile_flags_kernel<<<ceil_div(rows + 1, 256), 256, 0, s>>>(p.ro.get(), rows, breaks, window, short_max, rows_max,
+                                                              flags.get());
     VK_LAUNCH_CHECK();
     size_t tb = 0;
     VK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flags.get(), idx.get(), rows + 1, s));
@@ -153,13 +159,21 @@ void build_tiles(CsrPattern32 &p, cudaStream_t s, const unsigned char *breaks) {
     VK_CUDA(cudaMemcpyAsync(&last_flag, flags.get() + rows, sizeof(int), cudaMemcpyDeviceToHost, s));
     VK_CUDA(cudaStreamSynchronize(s));
     const int count = last_idx + last_flag; // number of boundaries (tiles + 1)
-    p.ntiles = count - 1;
-    p.tiles.reset(count);
-    tile_scatter_kernel<<<ceil_div(rows + 1, 256), 256, 0, s>>>(flags.get(), idx.get(), rows, p.tiles.get());
+    tiles.reset(count);
+    tile_scatter_kernel<<<ceil_div(rows + 1, 256), 256, 0, s>>>(flags.get(), idx.get(), rows, tiles.get());
     VK_LAUNCH_CHECK();
-    p.tile_k.reset(count);
-    tile_k_kernel<<<ceil_div(count, 256), 256, 0, s>>>(p.ro.get(), p.tiles.get(), count, p.tile_k.get());
+    tile_k.reset(count);
+    tile_k_kernel<<<ceil_div(count, 256), 256, 0, s>>>(p.ro.get(), tiles.get(), count, tile_k.get());
     VK_LAUNCH_CHECK();
+    VK_CUDA(cudaStreamSynchronize(s));
+    return count - 1;
+}
+} // namespace
+
+void build_tiles(CsrPattern32 &p, cudaStream_t s, const unsigned char *breaks) {
+    const int rows = p.rows;
+    p.ntiles = schedule(p, s, breaks, kChunk, kShortMax, kTileRows, p.tiles, p.tile_k);
+    p.nstiles = schedule(p, s, nullptr, kStageWindow, kStageShort, kStageRows, p.stiles, p.stile_k);
     // cost-balanced row ranges for the hybrid kernel
     int nnz_total = 0;
     VK_CUDA(cudaMemcpyAsync(&nnz_total, p.ro.get() + rows, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -276,10 +290,23 @@ template void gather_values<float, float>(const int *, const float *, float *, i
 
 // ---- autotuner ----------------------------------------------------------------
 namespace {
+// A stand-in for the fused passes: four per-row inputs loaded ahead of the
+// sums and a clamped update stored, so variants that run short of registers
+// with a real epilogue lose here too.
 template <class T>
-struct TuneEpi : EpiRow<T, TuneEpi<T>> {
+struct TuneEpi : EpiBase<T> {
     T *y;
-    __device__ void row(int i, const T (&s)[1], double (&)[1]) const { y[i] = s[0]; }
+    const T *a, *b, *lo, *hi;
+    struct Pre {
+        T a, b, lo, hi;
+    };
+    __device__ Pre load(int i) const { return Pre{a[i], b[i], lo[i], hi[i]}; }
+    template <int NV, int NR>
+    __device__ void row_pre(int i, const T (&s)[NV], const Pre &p, double (&red)[NR]) const {
+        const T v = clampbox(p.a * s[0] + p.b, p.lo, p.hi);
+        y[i] = v;
+        red[0] = smax(red[0], static_cast<double>(fabs(v - s[0])));
+    }
 };
 
 template <class T>
@@ -304,34 +331,40 @@ void autotune_pattern(CsrPattern32 &p, const T *val, cudaStream_t s, int64_t min
         return;
     }
     if (p.nnz < min_nnz || p.rows == 0 || p.cols == 0) return;
-    DevBuf<T> x(p.cols), y(p.rows);
+    DevBuf<T> x(p.cols), y(p.rows), pre(static_cast<size_t>(p.rows) * 4);
     fill_kernel<T><<<grid_for(p.cols), 256, 0, s>>>(x.get(), p.cols, T(1));
+    fill_kernel<T><<<grid_for(int64_t(p.rows) * 4), 256, 0, s>>>(pre.get(), int64_t(p.rows) * 4, T(1));
     VK_LAUNCH_CHECK();
     TuneEpi<T> e;
     e.y = y.get();
+    e.a = pre.get();
+    e.b = pre.get() + p.rows;
+    e.lo = pre.get() + 2 * static_cast<size_t>(p.rows);
+    e.hi = pre.get() + 3 * static_cast<size_t>(p.rows);
     cudaEvent_t a, b;
     VK_CUDA(cudaEventCreate(&a));
     VK_CUDA(cudaEventCreate(&b));
-    float best = 1e30f;
-    int best_v = 0;
+    // one untimed round, then the variants interleaved over rounds (clock
+    // drift hits them alike); each keeps its best round
+    float best[kFastVariants];
     for (int v = 0; v < kFastVariants; ++v) {
         p.variant = v;
-        const CsrView<T> M = view(p, val);
-        launch_tiles<T, T, 1, false>(M, Gathers<T, 1>{{x.get()}}, e, s); // warm-up
-        float times[3];
-        for (float &t : times) {
+        launch_tiles<T, T, 1, false>(view(p, val), Gathers<T, 1>{{x.get()}}, e, s);
+        best[v] = 1e30f;
+    }
+    for (int round = 0; round < kTuneRounds; ++round)
+        for (int v = 0; v < kFastVariants; ++v) {
+            p.variant = v;
+            const CsrView<T> M = view(p, val);
             VK_CUDA(cudaEventRecord(a, s));
             launch_tiles<T, T, 1, false>(M, Gathers<T, 1>{{x.get()}}, e, s);
             VK_CUDA(cudaEventRecord(b, s));
             VK_CUDA(cudaEventSynchronize(b));
+            float t = 0.f;
             VK_CUDA(cudaEventElapsedTime(&t, a, b));
+            best[v] = std::min(best[v], t);
         }
-        std::sort(times, times + 3);
-        if (times[1] < best) {
-            best = times[1];
-            best_v = v;
-        }
-    }
+    const int best_v = static_cast<int>(std::min_element(best, best + kFastVariants) - best);
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     p.variant = best_v;

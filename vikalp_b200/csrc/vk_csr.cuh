@@ -43,6 +43,19 @@ constexpr int kCap = kChunk + kShortMax;   // max nonzeros of a multi-row tile
 constexpr int kTileRows = 64;              // max rows per warp-tile
 constexpr int kPad = 8;                    // padding (elements) of index / value arrays
 constexpr int kMaxGridPerSM = 16;          // persistent CTAs per SM (upper bound)
+// The staged kernel's schedule: at most kStageRows rows whose starts fall in
+// one kStageWindow-sized window of the nonzero array, each at most
+// kStageShort long (so at most kStageCap nonzeros), or one longer row.
+constexpr int kStageWindow = 384;
+constexpr int kStageShort = 128;
+constexpr int kStageCap = kStageWindow + kStageShort; // 512
+constexpr int kStageRows = 32;
+constexpr int kStageSlots = kStageCap + 8; // staged elements per stage incl. the 16-byte widening
+// Dynamic shared memory of the staged kernel for value type T.
+template <class T>
+constexpr int stage_smem_bytes() {
+    return kWarps * 2 * kStageSlots * static_cast<int>(sizeof(int) + sizeof(T));
+}
 constexpr int kMaxGrid = 160 * kMaxGridPerSM; // partial-sum buffers are sized for this
 
 inline int64_t padded(int64_t nnz) { return nnz + kPad; }
@@ -54,7 +67,8 @@ struct CsrPattern32 {
     int64_t nnz = 0;
     DevBuf<int> ro, ci, tiles, tile_k;
     DevBuf<int> chunks; // cost-balanced row ranges for the hybrid kernel (nchunks+1 row starts)
-    int ntiles = 0, nchunks = 0;
+    DevBuf<int> stiles, stile_k; // the staged kernel's schedule (<= kStageRows rows, <= kStageCap nonzeros)
+    int ntiles = 0, nchunks = 0, nstiles = 0;
     int max_row = 0;
     int variant = 0; // FAST kernel variant picked by autotune_pattern
 };
@@ -73,15 +87,18 @@ struct CsrView {
     const int *__restrict__ tiles;
     const int *__restrict__ tile_k;
     const int *__restrict__ chunks;
+    const int *__restrict__ stiles;
+    const int *__restrict__ stile_k;
     int *err;
-    int rows, cols, ntiles, nchunks;
+    int rows, cols, ntiles, nchunks, nstiles;
     int variant; // FAST kernel variant (autotuned per matrix)
 };
 
 template <class T>
 inline CsrView<T> view(const CsrPattern32 &p, const T *val) {
-    return CsrView<T>{p.ro.get(), p.ci.get(), val, p.tiles.get(), p.tile_k.get(), p.chunks.get(), device_error_flag(),
-                      p.rows, p.cols, p.ntiles, p.nchunks, p.variant};
+    return CsrView<T>{p.ro.get(),         p.ci.get(),    val,      p.tiles.get(), p.tile_k.get(),
+                      p.chunks.get(),     p.stiles.get(), p.stile_k.get(), device_error_flag(), p.rows,
+                      p.cols,             p.ntiles,      p.nchunks, p.nstiles,     p.variant};
 }
 
 // Rounded multiply / add that the compiler never contracts into an FMA, so the
@@ -121,10 +138,13 @@ struct Gathers {
 //   HYB   > 0: the hybrid kernel (tile_kernel_hyb): a lane sums its own row
 //         when it has at most HYB nonzeros, longer rows are shared by
 //         sub-warps of SUB lanes (or by the whole warp)
+//   STAGE > 0: the staged kernel (tile_kernel_tma) with STAGE shared-memory
+//         stages per warp (HYB, SUB as in the hybrid kernel's row sums)
 struct FastVariant {
-    int u, pipe, minb, sub, hyb;
+    int u, pipe, minb, sub, hyb, stage = 0;
 };
-constexpr int kFastVariants = 11;
+constexpr int kFastVariants = 13;
+constexpr int kTuneRounds = 4; // timed rounds per variant in the autotuners
 __host__ __device__ constexpr FastVariant fast_variant(int v) {
     return v == 0   ? FastVariant{4, 1, 12, 0, 0}
            : v == 1 ? FastVariant{8, 1, 8, 0, 0}
@@ -136,7 +156,9 @@ __host__ __device__ constexpr FastVariant fast_variant(int v) {
            : v == 7 ? FastVariant{2, 0, 12, 16, 0}
            : v == 8 ? FastVariant{4, 0, 8, 8, 4}
            : v == 9 ? FastVariant{2, 0, 12, 8, 2}
-                    : FastVariant{2, 0, 12, 4, 4};
+           : v == 10 ? FastVariant{2, 0, 12, 4, 4}
+           : v == 11 ? FastVariant{8, 0, 4, 8, 8, 2}
+                     : FastVariant{4, 0, 4, 4, 4, 2};
 }
 
 template <class T, class A, int NV, class Epi, int U, bool PIPE, int MINB>
@@ -651,6 +673,206 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     epi.finish(red, scratch, blockIdx.x);
 }
 
+// Staged variant (sm_90+ bulk copies). Each warp runs its own two-stage
+// pipeline over the staged schedule (tiles of <= kStageRows rows and
+// <= kStageCap nonzeros, or one longer row taken in kStageCap pieces): one
+// lane issues cp.async.bulk copies of the next piece's column indices and
+// values (16-byte aligned: the piece is widened to whole 4-element groups,
+// inside the kPad padding) into shared memory, completing on an mbarrier,
+// while the warp works on the current piece. So the nonzero streams bypass
+// the L1 load path and only the random gathers of x (and the epilogue's
+// per-row inputs) go through it. Per piece: every lane loads its row's bounds
+// and epilogue inputs (one row per lane), the warp gathers x for all the
+// piece's nonzeros (U per lane in flight) and overwrites each staged value
+// with its product, then the row sums are read back from shared memory: a
+// lane sums its own row when it has at most S nonzeros, longer rows go to
+// sub-warps of L lanes or to the whole warp; each lane runs its row's
+// epilogue. A long row's pieces accumulate in a warp-wide carry. Waits are
+// bounded: a barrier that never completes sets the device error flag, the
+// warp stops taking work and waits (bounded) for its own copies in flight.
+// Not for epilogues that reduce per tile or skip tiles (they use the main
+// schedule's tile numbers); launch_fast gives those the hybrid kernel.
+template <class T, class A, int NV, class Epi, int S, int L, int U, int MINB>
+__global__ void __launch_bounds__(kTileThreads, MINB)
+    tile_kernel_tma(CsrView<T> M, Gathers<T, NV> g, Epi epi) {
+    static_assert(NV == 1 && sizeof(A) == sizeof(T), "products overwrite the staged values");
+    static_assert(L == 2 || L == 4 || L == 8 || L == 16, "sub-warp width");
+    if (epi.skip()) return;
+    constexpr int NR = Epi::NR;
+    constexpr int G = 32 / L;
+    constexpr int CAPR = kStageSlots;
+    using Pre = typename Epi::Pre;
+    // dynamic shared memory: [warp][stage][CAPR] indices, then values
+    extern __shared__ __align__(16) unsigned char stage_smem[];
+    auto s_ci = reinterpret_cast<int (*)[2][CAPR]>(stage_smem);
+    auto s_v = reinterpret_cast<T (*)[2][CAPR]>(stage_smem + sizeof(int) * kWarps * 2 * CAPR);
+    __shared__ alignas(8) uint64_t s_bar[kWarps][2];
+    __shared__ double scratch[32 * 8];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int sl = lane % L, sw = lane / L;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    uint64_t *bar = s_bar[warp];
+    if (lane == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    double red[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) red[r] = 0.0;
+    const A gs = epi.gscale(0);
+    const T *__restrict__ x = g.p[0];
+
+    const int W = gridDim.x * kWarps;
+    const int wid = blockIdx.x * kWarps + warp;
+    // the warp's pieces: tiles wid, wid + W, ...; a tile of n nonzeros has
+    // max(1, ceil(n / kStageCap)) pieces
+    auto next = [&](int &t, int &p) {
+        const int n = __ldg(M.stile_k + t + 1) - __ldg(M.stile_k + t);
+        if ((p + 1) * kStageCap < n) {
+            ++p;
+        } else {
+            t += W;
+            p = 0;
+        }
+    };
+    auto issue = [&](int st, int t, int p) {
+        if (lane == 0) {
+            const int a = __ldg(M.stile_k + t), b = __ldg(M.stile_k + t + 1);
+            const int k0 = a + p * kStageCap, k1 = min(b, k0 + kStageCap);
+            const int kb = k0 & ~3;
+            const int n = (k1 - kb + 3) & ~3;
+            mbar_arrive_expect_tx(&bar[st], static_cast<uint32_t>(n * (4 + sizeof(T))));
+            if (n > 0) {
+                bulk_g2s(s_ci[warp][st], M.ci + kb, static_cast<uint32_t>(n * 4), &bar[st]);
+                bulk_g2s(s_v[warp][st], M.val + kb, static_cast<uint32_t>(n * sizeof(T)), &bar[st]);
+            }
+        }
+    };
+
+    uint32_t phase[2] = {0u, 0u};
+    bool pending[2] = {false, false};
+    bool failed = false;
+    int t = wid, p = 0, st = 0;
+    A carry = A(0); // a long row's sum over its earlier pieces
+    if (t < M.nstiles) {
+        issue(0, t, 0);
+        pending[0] = true;
+    }
+    while (t < M.nstiles) {
+        int tn = t, pn = p;
+        next(tn, pn);
+        if (tn < M.nstiles) {
+            issue(st ^ 1, tn, pn);
+            pending[st ^ 1] = true;
+        }
+        const int r0 = __ldg(M.stiles + t), r1 = __ldg(M.stiles + t + 1);
+        const int a = __ldg(M.stile_k + t), b = __ldg(M.stile_k + t + 1);
+        const int k0 = a + p * kStageCap, k1 = min(b, k0 + kStageCap);
+        const bool last_piece = k1 == b;
+        const bool long_row = b - a > kStageCap; // one row in several pieces
+        // this piece's rows: bounds and epilogue inputs, one row per lane
+        const int r = r0 + lane;
+        const bool valid = !long_row && r < r1;
+        int ra = 0, rz = 0;
+        Pre pre{};
+        if (valid) {
+            ra = __ldg(M.ro + r);
+            rz = __ldg(M.ro + r + 1);
+            pre = epi.load(r);
+        } else if (long_row && lane == 0 && last_piece) {
+            pre = epi.load(r0);
+        }
+        if (!__all_sync(FULL, mbar_wait_bounded(&bar[st], phase[st]))) {
+            if (lane == 0) atomicCAS(M.err, 0, static_cast<int>(kDevErrBarrierTimeout));
+            failed = true;
+            break;
+        }
+        phase[st] ^= 1u;
+        pending[st] = false;
+        const int kb = k0 & ~3, off = k0 - kb, nz = k1 - k0;
+        const int *sc = s_ci[warp][st] + off;
+        T *sv = s_v[warp][st] + off;
+        // gathers: products over the staged values
+        for (int j = lane; j < nz; j += 32 * U) {
+            int c[U];
+            T xv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) c[u] = j + 32 * u < nz ? sc[j + 32 * u] : 0;
+#pragma unroll
+            for (int u = 0; u < U; ++u) xv[u] = j + 32 * u < nz ? __ldg(x + c[u]) : T(0);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (j + 32 * u < nz) sv[j + 32 * u] = static_cast<T>(static_cast<A>(sv[j + 32 * u]) * (gs * static_cast<A>(xv[u])));
+        }
+        __syncwarp();
+        if (long_row) {
+            A part = A(0);
+            for (int j = lane; j < nz; j += 32) part += static_cast<A>(sv[j]);
+            carry += warp_sum(part);
+            if (last_piece) {
+                if (lane == 0) {
+                    A s2[1] = {epi.init(r0, 0) + carry};
+                    epi.row_pre(r0, s2, pre, red);
+                }
+                carry = A(0);
+            }
+        } else {
+            // row sums from shared memory; local offsets relative to k0
+            const int la = ra - k0, len = rz - ra;
+            A sum = A(0);
+            if (valid && len <= S)
+                for (int j = 0; j < len; ++j) sum += static_cast<A>(sv[la + j]);
+            unsigned lm = __ballot_sync(FULL, valid && len > S);
+            while (lm) {
+                const int first = __ffs(lm) - 1;
+                const int fa = __shfl_sync(FULL, la, first), fl = __shfl_sync(FULL, len, first);
+                if (fl > 4 * L) {
+                    A part = A(0);
+                    for (int j = lane; j < fl; j += 32) part += static_cast<A>(sv[fa + j]);
+                    part = warp_sum(part);
+                    if (lane == first) sum = part;
+                    lm &= lm - 1u;
+                    continue;
+                }
+                const unsigned pos = __fns(lm, 0, sw + 1);
+                const bool has = pos < 32u;
+                const int src = has ? static_cast<int>(pos) : 0;
+                const int qa = __shfl_sync(FULL, la, src), ql = __shfl_sync(FULL, len, src);
+                A part = A(0);
+                if (has)
+                    for (int j = sl; j < ql; j += L) part += static_cast<A>(sv[qa + j]);
+#pragma unroll
+                for (int o = L / 2; o > 0; o >>= 1) part += __shfl_xor_sync(FULL, part, o, L);
+                const int rank = __popc(lm & lt_mask);
+                const bool mine = ((lm >> lane) & 1u) && rank < G;
+                const A tv = __shfl_sync(FULL, part, mine ? rank * L : 0);
+                if (mine) sum = tv;
+#pragma unroll
+                for (int i = 0; i < G; ++i) lm &= lm - 1u;
+            }
+            if (valid) {
+                A s2[1] = {epi.init(r, 0) + sum};
+                epi.row_pre(r, s2, pre, red);
+            }
+        }
+        // every lane is done with this stage before a copy overwrites it
+        fence_proxy_async_smem();
+        __syncwarp();
+        t = tn;
+        p = pn;
+        st ^= 1;
+    }
+    if (failed) {
+        // wait (bounded) for this warp's copies still in flight
+        for (int i = 0; i < 2; ++i)
+            if (pending[i]) mbar_wait_bounded(&bar[i], phase[i]);
+    }
+    epi.finish(red, scratch, blockIdx.x);
+}
+
 // Parity kernel: one thread per row, the reference's left-to-right order.
 template <class T, class A, int NV, class Epi>
 __global__ void __launch_bounds__(kTileThreads)
@@ -682,11 +904,11 @@ __global__ void __launch_bounds__(kTileThreads)
 }
 
 template <class K>
-inline int resident_grid(K kernel) {
+inline int resident_grid(K kernel, int smem = 0) {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kTileThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kTileThreads, smem);
     per = per < 1 ? 1 : (per > kMaxGridPerSM ? kMaxGridPerSM : per);
     const int r = sms * per;
     return r < kMaxGrid ? r : kMaxGrid;
@@ -696,16 +918,24 @@ template <class T, class A, int NV, class Epi, int V>
 inline int launch_fast(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi &epi, cudaStream_t s) {
     constexpr FastVariant fv = fast_variant(V);
     void (*kernel)(CsrView<T>, Gathers<T, NV>, Epi);
-    if constexpr (fv.hyb > 0)
+    constexpr bool staged_ok = NV == 1 && sizeof(A) == sizeof(T) && !Epi::kPerTile && !Epi::kSkipTiles;
+    if constexpr (fv.stage > 0 && staged_ok)
+        kernel = tile_kernel_tma<T, A, NV, Epi, fv.hyb, fv.sub, fv.u, fv.minb>;
+    else if constexpr (fv.hyb > 0)
         kernel = tile_kernel_hyb<T, A, NV, Epi, fv.hyb, fv.sub, fv.u, fv.minb>;
     else if constexpr (fv.sub > 0)
         kernel = tile_kernel_sub<T, A, NV, Epi, (fv.sub > 0 ? fv.sub : 32), fv.u, fv.minb>;
     else
         kernel = tile_kernel_fast<T, A, NV, Epi, fv.u, fv.pipe != 0, fv.minb>;
-    static const int resident = resident_grid(kernel);
-    const int need = (M.ntiles + kWarps - 1) / kWarps;
+    constexpr bool staged = fv.stage > 0 && staged_ok;
+    constexpr int smem = staged ? stage_smem_bytes<T>() : 0;
+    static const int resident = [&] {
+        if (smem > 0) VK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        return resident_grid(kernel, smem);
+    }();
+    const int need = ((staged ? M.nstiles : M.ntiles) + kWarps - 1) / kWarps;
     const int grid = need < resident ? (need > 0 ? need : 1) : resident;
-    kernel<<<grid, kTileThreads, 0, s>>>(M, g, epi);
+    kernel<<<grid, kTileThreads, smem, s>>>(M, g, epi);
     VK_LAUNCH_CHECK();
     return grid;
 }
@@ -736,6 +966,8 @@ inline int launch_tiles(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi 
     case 8: return launch_fast<T, A, NV, Epi, 8>(M, g, epi, s);
     case 9: return launch_fast<T, A, NV, Epi, 9>(M, g, epi, s);
     case 10: return launch_fast<T, A, NV, Epi, 10>(M, g, epi, s);
+    case 11: return launch_fast<T, A, NV, Epi, 11>(M, g, epi, s);
+    case 12: return launch_fast<T, A, NV, Epi, 12>(M, g, epi, s);
     default: return launch_fast<T, A, NV, Epi, 0>(M, g, epi, s);
     }
 }

@@ -656,57 +656,51 @@ private:
         cudaEvent_t a, b;
         VK_CUDA(cudaEventCreate(&a));
         VK_CUDA(cudaEventCreate(&b));
-        auto time_it = [&](auto &&launch) {
-            launch();
-            float t[3];
-            for (float &x : t) {
-                VK_CUDA(cudaEventRecord(a, s_));
-                launch();
-                VK_CUDA(cudaEventRecord(b, s_));
-                VK_CUDA(cudaEventSynchronize(b));
-                VK_CUDA(cudaEventElapsedTime(&x, a, b));
-            }
-            std::sort(t, t + 3);
-            return t[1];
-        };
         for (int pass = 0; pass < 2; ++pass) {
-            float best = 1e30f;
-            int best_v = 0;
-            for (int v = 0; v < kFastVariants; ++v) {
-                float ms;
+            auto launch = [&](int v) {
                 if (pass == 0) {
                     col_variant_ = v;
-                    ms = time_it([&] {
-                        if (dm_.qp) {
-                            RefColFastEpi<true> e;
-                            fill_col(e, x_[0].get());
-                            e.xn = x_[1].get();
-                            tiles(col_view(), Gathers<double, 1>{{y_.get()}}, e);
-                        } else {
-                            RefColFastEpi<false> e;
-                            fill_col(e, x_[0].get());
-                            e.xn = x_[1].get();
-                            tiles(col_view(), Gathers<double, 1>{{y_.get()}}, e);
-                        }
-                    });
+                    if (dm_.qp) {
+                        RefColFastEpi<true> e;
+                        fill_col(e, x_[0].get());
+                        e.xn = x_[1].get();
+                        tiles(col_view(), Gathers<double, 1>{{y_.get()}}, e);
+                    } else {
+                        RefColFastEpi<false> e;
+                        fill_col(e, x_[0].get());
+                        e.xn = x_[1].get();
+                        tiles(col_view(), Gathers<double, 1>{{y_.get()}}, e);
+                    }
                 } else {
                     row_variant_ = v;
-                    ms = time_it([&] {
-                        RefRowFastEpi r;
-                        r.ctl = ctl_.get();
-                        r.y = y_.get();
-                        r.kx = kx_.get();
-                        r.rl = srl_.get();
-                        r.ru = sru_.get();
-                        tiles(row_view(), Gathers<double, 1>{{x_[1].get()}}, r);
-                    });
+                    RefRowFastEpi r;
+                    r.ctl = ctl_.get();
+                    r.y = y_.get();
+                    r.kx = kx_.get();
+                    r.rl = srl_.get();
+                    r.ru = sru_.get();
+                    tiles(row_view(), Gathers<double, 1>{{x_[1].get()}}, r);
                 }
-                if (ms < best) {
-                    best = ms;
-                    best_v = v;
-                }
+            };
+            // one untimed round, then the variants interleaved over rounds
+            // (clock drift hits them alike); each keeps its best round
+            float best[kFastVariants];
+            for (int v = 0; v < kFastVariants; ++v) {
+                launch(v);
+                best[v] = 1e30f;
             }
-            (pass == 0 ? col_variant_ : row_variant_) = best_v;
+            for (int round = 0; round < kTuneRounds; ++round)
+                for (int v = 0; v < kFastVariants; ++v) {
+                    VK_CUDA(cudaEventRecord(a, s_));
+                    launch(v);
+                    VK_CUDA(cudaEventRecord(b, s_));
+                    VK_CUDA(cudaEventSynchronize(b));
+                    float ms = 0.f;
+                    VK_CUDA(cudaEventElapsedTime(&ms, a, b));
+                    best[v] = std::min(best[v], ms);
+                }
+            (pass == 0 ? col_variant_ : row_variant_) =
+                static_cast<int>(std::min_element(best, best + kFastVariants) - best);
         }
         cudaEventDestroy(a);
         cudaEventDestroy(b);
