@@ -135,9 +135,11 @@ def allmax(dist, v, local):
     return float(t.item())
 
 
-def profile_traffic():
-    """DRAM bytes per launch of the dominant kernel (the row pass) from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "row_pass_large_lp.md")
+def profile_traffic(kernel_name):
+    """DRAM bytes per launch of a fused pass (the column or the row pass of the
+    reference-scheme iteration on the large LP) from its committed ncu summary."""
+    name = "col_pass_large_lp.md" if kernel_name.startswith("column") else "row_pass_large_lp.md"
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
@@ -408,7 +410,7 @@ def main():
         dom = max(prof, key=lambda p: p["ms"] * p["launches"])
         achieved = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9
         line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                            "frac": round(achieved / peak, 4), "traffic": profile_traffic(),
+                            "frac": round(achieved / peak, 4), "traffic": profile_traffic(dom["name"]),
                             "kernel": f"{dom['name']} of the reference-scheme iteration (fp64, FAST order)",
                             "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                             "algorithmic_bytes": int(dom["bytes"]), "ms": round(dom["ms"], 4),

@@ -143,7 +143,7 @@ struct Gathers {
 struct FastVariant {
     int u, pipe, minb, sub, hyb, stage = 0;
 };
-constexpr int kFastVariants = 13;
+constexpr int kFastVariants = 15;
 constexpr int kTuneRounds = 4; // timed rounds per variant in the autotuners
 __host__ __device__ constexpr FastVariant fast_variant(int v) {
     return v == 0   ? FastVariant{4, 1, 12, 0, 0}
@@ -158,7 +158,9 @@ __host__ __device__ constexpr FastVariant fast_variant(int v) {
            : v == 9 ? FastVariant{2, 0, 12, 8, 2}
            : v == 10 ? FastVariant{2, 0, 12, 4, 4}
            : v == 11 ? FastVariant{8, 0, 4, 8, 8, 2}
-                     : FastVariant{4, 0, 4, 4, 4, 2};
+           : v == 12 ? FastVariant{4, 0, 4, 4, 4, 2}
+           : v == 13 ? FastVariant{2, 0, 16, 8, 2}
+                     : FastVariant{4, 0, 16, 4, 1};
 }
 
 template <class T, class A, int NV, class Epi, int U, bool PIPE, int MINB>
@@ -534,15 +536,10 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
 #pragma unroll
     for (int q = 0; q < NV; ++q) gs[q] = epi.gscale(q);
 
-    // rows [rb, re), re - rb <= 32
-    auto group = [&](int rb, int re) {
+    // rows [rb, re), re - rb <= 32; a, b: this lane's row bounds (0 when r >= re)
+    auto group = [&](int rb, int re, int a, int b) {
         const int r = rb + lane;
         const bool valid = r < re;
-        int a = 0, b = 0;
-        if (valid) {
-            a = __ldg(M.ro + r);
-            b = __ldg(M.ro + r + 1);
-        }
         Pre pre{};
         if (valid) pre = epi.load(r);
         const int len = b - a;
@@ -655,7 +652,15 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
         for (int tile = wid; tile < M.ntiles; tile += W) {
             if (epi.skip_tile(tile)) continue;
             const int r0 = __ldg(M.tiles + tile), r1 = __ldg(M.tiles + tile + 1);
-            for (int rb = r0; rb < r1; rb += 32) group(rb, rb + 32 < r1 ? rb + 32 : r1);
+            for (int rb = r0; rb < r1; rb += 32) {
+                const int re = rb + 32 < r1 ? rb + 32 : r1;
+                int a = 0, b = 0;
+                if (rb + lane < re) {
+                    a = __ldg(M.ro + rb + lane);
+                    b = __ldg(M.ro + rb + lane + 1);
+                }
+                group(rb, re, a, b);
+            }
             if constexpr (Epi::kPerTile) {
 #pragma unroll
                 for (int r = 0; r < NR; ++r) red[r] = warp_sum(red[r]);
@@ -667,7 +672,15 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
     } else {
         for (int ch = wid; ch < M.nchunks; ch += W) {
             const int r0 = __ldg(M.chunks + ch), r1 = __ldg(M.chunks + ch + 1);
-            for (int rb = r0; rb < r1; rb += 32) group(rb, rb + 32 < r1 ? rb + 32 : r1);
+            for (int rb = r0; rb < r1; rb += 32) {
+                const int re = rb + 32 < r1 ? rb + 32 : r1;
+                int a = 0, b = 0;
+                if (rb + lane < re) {
+                    a = __ldg(M.ro + rb + lane);
+                    b = __ldg(M.ro + rb + lane + 1);
+                }
+                group(rb, re, a, b);
+            }
         }
     }
     epi.finish(red, scratch, blockIdx.x);
@@ -968,6 +981,9 @@ inline int launch_tiles(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi 
     case 10: return launch_fast<T, A, NV, Epi, 10>(M, g, epi, s);
     case 11: return launch_fast<T, A, NV, Epi, 11>(M, g, epi, s);
     case 12: return launch_fast<T, A, NV, Epi, 12>(M, g, epi, s);
+    case 13: return launch_fast<T, A, NV, Epi, 13>(M, g, epi, s);
+    case 14: return launch_fast<T, A, NV, Epi, 14>(M, g, epi, s);
+
     default: return launch_fast<T, A, NV, Epi, 0>(M, g, epi, s);
     }
 }
