@@ -155,6 +155,14 @@ std::string validate_problem(const vk_problem &p, const vk_options &o, bool &uns
     return "";
 }
 
+void ensure_tuned(DeviceModel &dm, cudaStream_t s) {
+    if (dm.tuned) return;
+    autotune_pattern<double>(dm.a, dm.a_val.get(), s);
+    autotune_pattern<double>(dm.at, dm.at_val.get(), s);
+    if (dm.qp) autotune_pattern<double>(dm.q, dm.q_val.get(), s);
+    dm.tuned = true;
+}
+
 std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s) {
     auto dm = std::make_unique<DeviceModel>();
     const int64_t m = p.A.rows, n = p.A.cols;
@@ -172,8 +180,6 @@ std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s) {
     transpose_pattern(dm->a, dm->at, dm->perm, s);
     dm->at_val.reset(padded(dm->nnz));
     gather_values<double, double>(dm->perm.get(), dm->a_val.get(), dm->at_val.get(), dm->nnz, s);
-    autotune_pattern<double>(dm->a, dm->a_val.get(), s);
-    autotune_pattern<double>(dm->at, dm->at_val.get(), s);
     if (dm->qp) {
         upload_pattern(n, n, p.Q.row_offsets, p.Q.col_indices, dm->q, s);
         dm->q_val.reset(padded(dm->q_nnz));
@@ -181,7 +187,6 @@ std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s) {
         dm->h_qro.assign(p.Q.row_offsets, p.Q.row_offsets + n + 1);
         dm->h_qci.assign(p.Q.col_indices, p.Q.col_indices + dm->q_nnz);
         dm->h_qv.assign(p.Q.values, p.Q.values + dm->q_nnz);
-        autotune_pattern<double>(dm->q, dm->q_val.get(), s);
     }
     auto up = [&](DevBuf<double> &b, const double *h, int64_t k) {
         b.reset(k > 0 ? k : 1);
@@ -367,9 +372,18 @@ Solver::Solver(const vk_problem &p, const vk_options &o) : opts_(o) {
     VK_CUDA(cudaSetDevice(o.device));
     device_error_flag(); // allocated here, never inside a graph capture
     VK_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    PhaseLog log(o.verbose, "create", stream_);
     dm_ = upload_model(p, stream_);
+    log.mark("upload + transpose");
+    // the Halpern passes (and the reference scheme's Q pass) run on the
+    // patterns' tuned variants; the reference scheme tunes its fused passes itself
+    if (o.algorithm == VK_ALGO_HALPERN || dm_->qp) {
+        ensure_tuned(*dm_, stream_);
+        log.mark("pattern autotune");
+    }
     engine_ = o.algorithm == VK_ALGO_HALPERN ? make_halpern_engine(*dm_, o, stream_)
                                              : make_reference_engine(*dm_, o, stream_);
+    log.mark("engine setup");
 }
 
 std::string Solver::set_options(const vk_options &o) {
@@ -458,7 +472,10 @@ void Solver::solve(const double *warm, const double *lo_ovr, const double *hi_ov
 
     DevBuf<double> xo(n), yo(m > 0 ? m : 1);
     RunInfo info;
+    PhaseLog log(opts_.verbose, "solve", s);
+    log.mark("checks + overrides");
     engine_->run(warm ? dwarm.get() : nullptr, lo.get(), hi.get(), xo.get(), yo.get(), info, started);
+    log.mark("iterations");
 
     // post-processing
     const bool exact = opts_.spmv_order == VK_SPMV_SEQUENTIAL;
@@ -577,6 +594,7 @@ void Solver::solve(const double *warm, const double *lo_ovr, const double *hi_ov
     }
     r->status = status;
     r->solve_seconds = seconds_since(started);
+    log.mark("post-processing + results");
 }
 
 } // namespace vk

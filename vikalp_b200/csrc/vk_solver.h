@@ -25,6 +25,7 @@ struct DeviceModel {
     std::vector<int64_t> h_qro, h_qci;       // Q on the host (objective's quadratic term)
     std::vector<double> h_qv;
     std::vector<double> h_vl, h_vu;          // model bounds (override validation)
+    bool tuned = false;                      // pattern variants timed (ensure_tuned)
 };
 
 // Device control block of the reference scheme (pdhg.cpp:75-150).
@@ -68,8 +69,11 @@ private:
 // SolveStatus::UnsupportedModel instead of InvalidModel.
 std::string validate_problem(const vk_problem &p, const vk_options &o, bool &unsupported);
 
-// Uploads a validated problem.
+// Uploads a validated problem. The sparse-pass variants of its patterns are
+// timed on first need (ensure_tuned): engines whose passes use the patterns'
+// variants call it; the reference scheme tunes its own two fused passes.
 std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s);
+void ensure_tuned(DeviceModel &dm, cudaStream_t s);
 
 // Independent LPs solved together (vk_batch.cu); throws on invalid input.
 void batch_solve(const vk_problem *problems, int count, const vk_options &o, vk_result *results);
