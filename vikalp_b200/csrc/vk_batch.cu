@@ -206,17 +206,19 @@ __global__ void segment_reduce_kernel(const double *__restrict__ partials, const
     }
 }
 
-// out[b] = sum_{i in segment b} a_i * a_i (contiguous segments; one warp each).
+// out[b] = sum_{i in segment b} a_i * a_i (contiguous segments; one block
+// each, fixed reduction tree, so deterministic).
 template <class T>
 __global__ void segment_norm2_kernel(const T *__restrict__ a, const int *__restrict__ off, int count,
                                      double *__restrict__ out) {
-    const int b = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
+    __shared__ double scratch[32];
+    const int b = blockIdx.x;
     if (b >= count) return;
-    double s = 0.0;
-    for (int i = off[b] + lane; i < off[b + 1]; i += 32) s += static_cast<double>(a[i]) * static_cast<double>(a[i]);
-    s = warp_sum(s);
-    if (lane == 0) out[b] = s;
+    double s[1] = {0.0};
+    for (int i = off[b] + threadIdx.x; i < off[b + 1]; i += blockDim.x)
+        s[0] += static_cast<double>(a[i]) * static_cast<double>(a[i]);
+    block_sum<1>(s, scratch);
+    if (threadIdx.x == 0) out[b] = s[0];
 }
 
 template <class T>
@@ -391,6 +393,8 @@ class BatchEngine {
     friend class SharedEngine; // reuses the scaled model of a one-instance batch
 
 public:
+    // the objective vector in original units, concatenated over the instances
+    const double *c_orig() const { return c_orig_.get(); }
     BatchEngine(const vk_problem *probs, int count, const vk_options &o) : o_(o), B_(count) {
         VK_CUDA(cudaSetDevice(o.device));
         device_error_flag();
@@ -591,6 +595,9 @@ private:
         const DevBuf<double> &at_val = at_val_;
         DevBuf<double> c, vl, vu, rl, ru;
         up(c, h_c_);
+        c_orig_.reset(n_ > 0 ? n_ : 1);
+        if (n_ > 0)
+            VK_CUDA(cudaMemcpyAsync(c_orig_.get(), c.get(), n_ * sizeof(double), cudaMemcpyDeviceToDevice, s_));
         up(vl, h_vl_);
         up(vu, h_vu_);
         up(rl, h_rl_);
@@ -694,8 +701,7 @@ private:
         up(coff, col_off_);
         bseed_kernel<<<grid1d(n), 256, 0, s_>>>(v.get(), cinst_.get(), coff.get(), n);
         VK_LAUNCH_CHECK();
-        const int wb = ceil_div(int64_t(B_) * 32, 256);
-        segment_norm2_kernel<double><<<wb, 256, 0, s_>>>(v.get(), coff.get(), B_, nrm.get());
+        segment_norm2_kernel<double><<<B_, 256, 0, s_>>>(v.get(), coff.get(), B_, nrm.get());
         segment_scale_kernel<double><<<grid1d(n), 256, 0, s_>>>(v.get(), cinst_.get(), n, nrm.get());
         // Each instance keeps the estimate of the iteration at which its own
         // sequence settled (the single-instance stopping rule); the shared
@@ -710,7 +716,7 @@ private:
                 BStore<double> ez;
                 ez.y = z.get();
                 launch_tiles<double, double, 1, false>(view(at_, s64_.kat.get()), Gathers<double, 1>{{w.get()}}, ez, s_);
-                segment_norm2_kernel<double><<<wb, 256, 0, s_>>>(z.get(), coff.get(), B_, nrm.get());
+                segment_norm2_kernel<double><<<B_, 256, 0, s_>>>(z.get(), coff.get(), B_, nrm.get());
                 VK_CUDA(cudaMemcpyAsync(h.data(), nrm.get(), B_ * 8, cudaMemcpyDeviceToHost, s_));
                 VK_CUDA(cudaStreamSynchronize(s_));
                 segment_scale_kernel<double><<<grid1d(n), 256, 0, s_>>>(z.get(), cinst_.get(), n, nrm.get());
@@ -951,6 +957,7 @@ private:
     DevBuf<int> perm_, rinst_, cinst_, tinst_a_, tinst_at_, tbeg_a_, tbeg_at_;
     DevBuf<double> a_val_, at_val_; // original values (setup only)
     DevBuf<double> rs_, cs_;
+    DevBuf<double> c_orig_;
     BState<double> s64_;
     BState<float> s32_;
     DevBuf<double> eta_, omega_, tau_, sigma_, rr_, rp_, bn_, cn_, off_, kkt_, relp_, reld_, relg_;
@@ -1263,63 +1270,70 @@ struct SpmmMat {
 // One pass: for every row i and instance b, s = sum_k val_k * X[ci_k * ld + b],
 // handed to the epilogue. blockIdx.x = p * G + g: group g of 32*VEC instances,
 // block p of the P blocks serving that group (rows p*8 + warp, stride P*8).
+// One pass of the shared matrix for every instance group: block p takes rows
+// p*kSpmmWarps + warp, stepping by gridDim.x*kSpmmWarps, and walks the
+// instance groups g = 0..G-1 in order, so all blocks gather from one group's
+// slice of X (n * 32 * VEC values) at a time and that slice stays in L2.
 template <class T, int VEC, class Epi>
 __global__ void __launch_bounds__(kSpmmWarps * 32, 3)
     spmm_kernel(SpmmMat<T> M, const T *__restrict__ X, int ld, int G, Epi epi, double *__restrict__ partials) {
     constexpr int NR = Epi::NR;
-    const int g = blockIdx.x % G, p = blockIdx.x / G, P = gridDim.x / G;
+    const int p = blockIdx.x, P = gridDim.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b0 = g * 32 * VEC + lane * VEC;
-    const typename Epi::Lane L = epi.lane(b0);
-    double red[kSpmmMaxR][VEC];
+    for (int g = 0; g < G; ++g) {
+        const int b0 = g * 32 * VEC + lane * VEC;
+        const typename Epi::Lane L = epi.lane(b0);
+        double red[kSpmmMaxR][VEC];
 #pragma unroll
-    for (int r = 0; r < kSpmmMaxR; ++r)
+        for (int r = 0; r < kSpmmMaxR; ++r)
 #pragma unroll
-        for (int q = 0; q < VEC; ++q) red[r][q] = 0.0;
-    const T *Xb = X + b0;
-    for (int i = p * kSpmmWarps + warp; i < M.rows; i += P * kSpmmWarps) {
-        const int k0 = __ldg(M.ro + i), k1 = __ldg(M.ro + i + 1);
-        T acc[VEC];
+            for (int q = 0; q < VEC; ++q) red[r][q] = 0.0;
+        const T *Xb = X + b0;
+        for (int i = p * kSpmmWarps + warp; i < M.rows; i += P * kSpmmWarps) {
+            const int k0 = __ldg(M.ro + i), k1 = __ldg(M.ro + i + 1);
+            T acc[VEC];
 #pragma unroll
-        for (int q = 0; q < VEC; ++q) acc[q] = T(0);
-        int k = k0;
-        for (; k + 4 <= k1; k += 4) {
-            int cc[4];
-            T vv[4], xv[4][VEC];
+            for (int q = 0; q < VEC; ++q) acc[q] = T(0);
+            int k = k0;
+            for (; k + 4 <= k1; k += 4) {
+                int cc[4];
+                T vv[4], xv[4][VEC];
 #pragma unroll
-            for (int t = 0; t < 4; ++t) {
-                cc[t] = __ldg(M.ci + k + t);
-                vv[t] = __ldg(M.val + k + t);
+                for (int t = 0; t < 4; ++t) {
+                    cc[t] = __ldg(M.ci + k + t);
+                    vv[t] = __ldg(M.val + k + t);
+                }
+#pragma unroll
+                for (int t = 0; t < 4; ++t) ldg_vec<T, VEC>(Xb + static_cast<size_t>(cc[t]) * ld, xv[t]);
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) acc[q] += vv[t] * xv[t][q];
             }
+            for (; k < k1; ++k) {
+                const int cc = __ldg(M.ci + k);
+                const T vv = __ldg(M.val + k);
+                T xv[VEC];
+                ldg_vec<T, VEC>(Xb + static_cast<size_t>(cc) * ld, xv);
 #pragma unroll
-            for (int t = 0; t < 4; ++t) ldg_vec<T, VEC>(Xb + static_cast<size_t>(cc[t]) * ld, xv[t]);
-#pragma unroll
-            for (int t = 0; t < 4; ++t)
-#pragma unroll
-                for (int q = 0; q < VEC; ++q) acc[q] += vv[t] * xv[t][q];
+                for (int q = 0; q < VEC; ++q) acc[q] += vv * xv[q];
+            }
+            epi.row(i, b0, L, acc, red);
         }
-        for (; k < k1; ++k) {
-            const int cc = __ldg(M.ci + k);
-            const T vv = __ldg(M.val + k);
-            T xv[VEC];
-            ldg_vec<T, VEC>(Xb + static_cast<size_t>(cc) * ld, xv);
+        if constexpr (NR > 0) {
+            __shared__ double sred[kSpmmWarps][NR][32 * VEC];
 #pragma unroll
-            for (int q = 0; q < VEC; ++q) acc[q] += vv * xv[q];
-        }
-        epi.row(i, b0, L, acc, red);
-    }
-    if constexpr (NR > 0) {
-        __shared__ double sred[kSpmmWarps][NR][32 * VEC];
+            for (int r = 0; r < NR; ++r)
 #pragma unroll
-        for (int r = 0; r < NR; ++r)
-#pragma unroll
-            for (int q = 0; q < VEC; ++q) sred[warp][r][lane * VEC + q] = red[r][q];
-        __syncthreads();
-        for (int e = threadIdx.x; e < NR * 32 * VEC; e += blockDim.x) {
-            const int r = e / (32 * VEC), t = e % (32 * VEC);
-            double acc = 0.0;
-            for (int w = 0; w < kSpmmWarps; ++w) acc += sred[w][r][t];
-            partials[(static_cast<size_t>(p) * NR + r) * ld + g * 32 * VEC + t] = acc;
+                for (int q = 0; q < VEC; ++q) sred[warp][r][lane * VEC + q] = red[r][q];
+            __syncthreads();
+            for (int e = threadIdx.x; e < NR * 32 * VEC; e += blockDim.x) {
+                const int r = e / (32 * VEC), t = e % (32 * VEC);
+                double acc = 0.0;
+                for (int w = 0; w < kSpmmWarps; ++w) acc += sred[w][r][t];
+                partials[(static_cast<size_t>(p) * NR + r) * ld + g * 32 * VEC + t] = acc;
+            }
+            __syncthreads(); // sred is refilled by the next group
         }
     }
 }
@@ -1395,6 +1409,18 @@ __global__ void soverride_kernel(const double *__restrict__ lo, const double *__
     ovu[e] = u;
 }
 
+// out[b] = sum_j c[j] * x[b * n + j] (one block per instance, fixed tree).
+__global__ void sobjective_kernel(const double *__restrict__ x, const double *__restrict__ c, int n,
+                                  double *__restrict__ out) {
+    __shared__ double scratch[32];
+    const int b = blockIdx.x;
+    const double *xb = x + static_cast<size_t>(b) * n;
+    double s[1] = {0.0};
+    for (int j = threadIdx.x; j < n; j += blockDim.x) s[0] += c[j] * xb[j];
+    block_sum<1>(s, scratch);
+    if (threadIdx.x == 0) out[b] = s[0];
+}
+
 // out[b * n + j] = a[j * ld + b] * s[j]: unscale and de-interleave.
 __global__ void sunscale_kernel(const double *__restrict__ a, const double *__restrict__ s, int n, int count, int ld,
                                 double *__restrict__ out) {
@@ -1425,8 +1451,9 @@ public:
         vec32_ = B_ >= 128 ? 4 : 1;
         vec64_ = (B_ >= 64 && ld_ % 64 == 0) ? 2 : 1;
         const int sms = sm_count();
-        P32_ = std::max(1, 4 * sms / (ld_ / (32 * vec32_)));
-        P64_ = std::max(1, 4 * sms / (ld_ / (32 * vec64_)));
+        // one resident wave of blocks; each walks every instance group
+        P32_ = 4 * sms;
+        P64_ = 4 * sms;
         control_arrays();
         pmax_ = std::max(P32_, P64_);
         partial_.reset(static_cast<size_t>(pmax_) * kSpmmMaxR * ld_);
@@ -1602,11 +1629,22 @@ public:
         if (m > 0)
             sunscale_kernel<<<grid_for64(static_cast<int64_t>(B_) * m), 256, 0, s_>>>(
                 s64_.yhat.get(), base_.rs_.get(), m, B_, ld_, yo.get());
+        // objectives on the device (one block per instance), then x and y
+        // straight into the caller's arrays
+        DevBuf<double> dobj(B_);
+        sobjective_kernel<<<B_, 256, 0, s_>>>(xo.get(), base_.c_orig(), n, dobj.get());
         VK_LAUNCH_CHECK();
-        std::vector<double> hx(bn), hy(static_cast<size_t>(B_) * m);
-        VK_CUDA(cudaMemcpyAsync(hx.data(), xo.get(), bn * sizeof(double), cudaMemcpyDeviceToHost, s_));
-        if (m > 0)
-            VK_CUDA(cudaMemcpyAsync(hy.data(), yo.get(), hy.size() * sizeof(double), cudaMemcpyDeviceToHost, s_));
+        std::vector<double> hobj(B_);
+        VK_CUDA(cudaMemcpyAsync(hobj.data(), dobj.get(), B_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
+        for (int b = 0; b < B_; ++b) {
+            if (invalid[b]) continue;
+            if (results[b].x)
+                VK_CUDA(cudaMemcpyAsync(results[b].x, xo.get() + static_cast<size_t>(b) * n, n * sizeof(double),
+                                        cudaMemcpyDeviceToHost, s_));
+            if (results[b].y && m > 0)
+                VK_CUDA(cudaMemcpyAsync(results[b].y, yo.get() + static_cast<size_t>(b) * m, m * sizeof(double),
+                                        cudaMemcpyDeviceToHost, s_));
+        }
         VK_CUDA(cudaStreamSynchronize(s_));
         lg.mark("results to host");
         const double secs = seconds_since(started);
@@ -1626,12 +1664,7 @@ public:
                     std::numeric_limits<double>::quiet_NaN();
                 continue;
             }
-            const double *xb = hx.data() + static_cast<size_t>(b) * n;
-            if (r.x) std::copy(xb, xb + n, r.x);
-            if (r.y && m > 0) std::copy(hy.begin() + static_cast<size_t>(b) * m, hy.begin() + static_cast<size_t>(b + 1) * m, r.y);
-            double obj = model_.objective_offset;
-            for (int j = 0; j < n; ++j) obj += model_.c[j] * xb[j];
-            r.objective = obj;
+            r.objective = model_.objective_offset + hobj[b];
             r.status = h_done_[b] ? h_status_[b] : (timed_out ? VK_STATUS_TIME_LIMIT : VK_STATUS_ITERATION_LIMIT);
             r.iterations = h_iters_[b];
             r.restarts = h_restarts_[b];
@@ -1818,7 +1851,7 @@ private:
         const int P = std::is_same<T, double>::value ? P64_ : P32_;
         const SpmmMat<T> M = mat<T>(transposed);
         if (M.rows == 0) return;
-        spmm_kernel<T, VEC, Epi><<<G * P, kSpmmWarps * 32, 0, s_>>>(M, X, ld_, G, e, partial_.get());
+        spmm_kernel<T, VEC, Epi><<<P, kSpmmWarps * 32, 0, s_>>>(M, X, ld_, G, e, partial_.get());
         VK_LAUNCH_CHECK();
     }
 

@@ -472,12 +472,16 @@ public:
         mixed_ = o.precision == VK_PREC_MIXED;
         chunk_ = std::max(2, o.check_every > 0 ? o.check_every : 64);
         const int m = dm.m, n = dm.n;
+        PhaseLog log(o.verbose, "halpern setup", s);
         rs_.reset(m > 0 ? m : 1);
         cs_.reset(n);
         compute_scaling();
+        log.mark("scaling");
         setup_state(s64_);
         if (mixed_) setup_state(s32_);
+        log.mark("scaled state");
         step_size();
+        log.mark("step size (power iteration)");
         ctl_.reset(1);
         hctl_.reset(1);
         pc_.reset(static_cast<size_t>(kMaxGrid) * kColCheckSums);
