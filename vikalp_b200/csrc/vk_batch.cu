@@ -1117,11 +1117,23 @@ struct SColEpi {
         }
         return L;
     }
-    __device__ void row(int j, int b0, const Lane &L, const T (&s)[VEC], double (&red)[kSpmmMaxR][VEC]) const {
+    // the iterate and the anchor, loaded before the row's gathers
+    struct Pre {
+        T x[VEC], x0[VEC];
+    };
+    __device__ Pre pre(int j, int b0) const {
         const size_t at = static_cast<size_t>(j) * ld + b0;
-        T xv[VEC], x0v[VEC], lo[VEC], hi[VEC], xh[VEC], xb[VEC], xn[VEC];
-        ld_vec<T, VEC>(x + at, xv);
-        ld_vec<T, VEC>(x0 + at, x0v);
+        Pre p;
+        ld_vec<T, VEC>(x + at, p.x);
+        ld_vec<T, VEC>(x0 + at, p.x0);
+        return p;
+    }
+    __device__ void row(int j, int b0, const Lane &L, const T (&s)[VEC], double (&red)[kSpmmMaxR][VEC],
+                        const Pre &p) const {
+        const size_t at = static_cast<size_t>(j) * ld + b0;
+        T lo[VEC], hi[VEC], xh[VEC], xb[VEC], xn[VEC];
+        const T(&xv)[VEC] = p.x;
+        const T(&x0v)[VEC] = p.x0;
         col_bounds<T, VEC>(j, b0, ld, l, u, ovr, ovl, ovu, lo, hi);
         const T cj = __ldg(c + j);
 #pragma unroll
@@ -1163,12 +1175,27 @@ struct SRowEpi {
         }
         return L;
     }
-    __device__ void row(int i, int b0, const Lane &L, const T (&s)[VEC], double (&red)[kSpmmMaxR][VEC]) const {
+    // the iterate, the anchor and the row bounds, loaded before the row's gathers
+    struct Pre {
+        T y[VEC], y0[VEC];
+        T lo, hi;
+    };
+    __device__ Pre pre(int i, int b0) const {
         const size_t at = static_cast<size_t>(i) * ld + b0;
-        T yv[VEC], y0v[VEC], yh[VEC], yn[VEC];
-        ld_vec<T, VEC>(y + at, yv);
-        ld_vec<T, VEC>(y0 + at, y0v);
-        const T lo = __ldg(rl + i), hi = __ldg(ru + i);
+        Pre p;
+        ld_vec<T, VEC>(y + at, p.y);
+        ld_vec<T, VEC>(y0 + at, p.y0);
+        p.lo = __ldg(rl + i);
+        p.hi = __ldg(ru + i);
+        return p;
+    }
+    __device__ void row(int i, int b0, const Lane &L, const T (&s)[VEC], double (&red)[kSpmmMaxR][VEC],
+                        const Pre &p) const {
+        const size_t at = static_cast<size_t>(i) * ld + b0;
+        T yh[VEC], yn[VEC];
+        const T(&yv)[VEC] = p.y;
+        const T(&y0v)[VEC] = p.y0;
+        const T lo = p.lo, hi = p.hi;
 #pragma unroll
         for (int q = 0; q < VEC; ++q) {
             const T v = yv[q] + L.sigma[q] * s[q];
@@ -1199,7 +1226,10 @@ struct SKktRowEpi {
         lane_activity<T, VEC>(ctl, b0, L);
         return L;
     }
-    __device__ void row(int i, int b0, const Lane &L, const T (&s)[VEC], double (&red)[kSpmmMaxR][VEC]) const {
+    struct Pre {};
+    __device__ Pre pre(int, int) const { return Pre{}; }
+    __device__ void row(int i, int b0, const Lane &L, const T (&s)[VEC], double (&red)[kSpmmMaxR][VEC],
+                        const Pre &) const {
         T yv[VEC];
         ld_vec<T, VEC>(yhat + static_cast<size_t>(i) * ld + b0, yv);
         const double lo = static_cast<double>(__ldg(rl + i)), hi = static_cast<double>(__ldg(ru + i));
@@ -1235,7 +1265,10 @@ struct SKktColEpi {
         lane_activity<T, VEC>(ctl, b0, L);
         return L;
     }
-    __device__ void row(int j, int b0, const Lane &L, const T (&s)[VEC], double (&red)[kSpmmMaxR][VEC]) const {
+    struct Pre {};
+    __device__ Pre pre(int, int) const { return Pre{}; }
+    __device__ void row(int j, int b0, const Lane &L, const T (&s)[VEC], double (&red)[kSpmmMaxR][VEC],
+                        const Pre &) const {
         T xv[VEC], lo[VEC], hi[VEC];
         ld_vec<T, VEC>(xhat + static_cast<size_t>(j) * ld + b0, xv);
         col_bounds<T, VEC>(j, b0, ld, l, u, ovr, ovl, ovu, lo, hi);
@@ -1273,7 +1306,8 @@ struct SpmmMat {
 // One pass of the shared matrix for every instance group: block p takes rows
 // p*kSpmmWarps + warp, stepping by gridDim.x*kSpmmWarps, and walks the
 // instance groups g = 0..G-1 in order, so all blocks gather from one group's
-// slice of X (n * 32 * VEC values) at a time and that slice stays in L2.
+// slice of X (n * 32 * VEC values) at a time and that slice stays in L2. A
+// group whose instances have all stopped is skipped.
 template <class T, int VEC, class Epi>
 __global__ void __launch_bounds__(kSpmmWarps * 32, 3)
     spmm_kernel(SpmmMat<T> M, const T *__restrict__ X, int ld, int G, Epi epi, double *__restrict__ partials) {
@@ -1289,8 +1323,15 @@ __global__ void __launch_bounds__(kSpmmWarps * 32, 3)
 #pragma unroll
             for (int q = 0; q < VEC; ++q) red[r][q] = 0.0;
         const T *Xb = X + b0;
-        for (int i = p * kSpmmWarps + warp; i < M.rows; i += P * kSpmmWarps) {
+        // the warp's lanes cover the whole group: skip its rows when every
+        // instance of the group has stopped (the partials below stay zero)
+        bool mine = false;
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) mine = mine || L.act[q];
+        const int rows = __any_sync(0xffffffffu, mine) ? M.rows : 0;
+        for (int i = p * kSpmmWarps + warp; i < rows; i += P * kSpmmWarps) {
             const int k0 = __ldg(M.ro + i), k1 = __ldg(M.ro + i + 1);
+            const typename Epi::Pre pre = epi.pre(i, b0);
             T acc[VEC];
 #pragma unroll
             for (int q = 0; q < VEC; ++q) acc[q] = T(0);
@@ -1318,7 +1359,7 @@ __global__ void __launch_bounds__(kSpmmWarps * 32, 3)
 #pragma unroll
                 for (int q = 0; q < VEC; ++q) acc[q] += vv * xv[q];
             }
-            epi.row(i, b0, L, acc, red);
+            epi.row(i, b0, L, acc, red, pre);
         }
         if constexpr (NR > 0) {
             __shared__ double sred[kSpmmWarps][NR][32 * VEC];
@@ -1962,8 +2003,13 @@ void batch_solve(const vk_problem *probs, int count, const vk_options &o, vk_res
     }
     if (m >= (int64_t(1) << 31) || n >= (int64_t(1) << 31) || nnz >= (int64_t(1) << 31))
         throw Unsupported("the batch exceeds the int32 index range of the device structures");
-    BatchEngine eng(probs, count, o);
-    eng.solve(results);
+    const auto t0 = std::chrono::steady_clock::now();
+    {
+        BatchEngine eng(probs, count, o);
+        eng.solve(results);
+    }
+    if (o.verbose > 0)
+        std::fprintf(stderr, "[vikalp_b200] batch: total incl. release       %8.3f s\n", seconds_since(t0));
 }
 
 
@@ -1984,8 +2030,13 @@ void batch_solve_shared(const vk_problem &p, int count, const double *lower, con
     const int64_t ld = (static_cast<int64_t>(count) + 127) / 128 * 128;
     if ((p.A.cols + 1) * ld >= (int64_t(1) << 40) || count >= (1 << 24))
         throw Unsupported("the batch is too large for one device");
-    SharedEngine eng(p, count, o);
-    eng.solve(lower, upper, warm, results);
+    const auto t0 = std::chrono::steady_clock::now();
+    {
+        SharedEngine eng(p, count, o);
+        eng.solve(lower, upper, warm, results);
+    }
+    if (o.verbose > 0)
+        std::fprintf(stderr, "[vikalp_b200] shared: total incl. release      %8.3f s\n", seconds_since(t0));
 }
 
 } // namespace vk
