@@ -145,8 +145,12 @@ int vk_pdhg_create(const vk_problem *problem, const vk_options *opts, vk_pdhg **
         else
             vk_default_options(&o);
         bool unsupported = false;
+        const auto t0 = std::chrono::steady_clock::now();
         const std::string msg = vk::validate_problem(*problem, o, unsupported);
         if (!msg.empty()) return set_error(unsupported ? VK_ERR_UNSUPPORTED : VK_ERR_INVALID, msg);
+        if (o.verbose > 0)
+            std::fprintf(stderr, "[vikalp_b200] create: %-28s %8.3f s\n", "validation (host)",
+                         std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
         auto h = std::make_unique<vk_pdhg>();
         h->solver = std::make_unique<vk::Solver>(*problem, o);
         *out = h.release();

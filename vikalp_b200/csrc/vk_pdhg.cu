@@ -163,7 +163,8 @@ void ensure_tuned(DeviceModel &dm, cudaStream_t s) {
     dm.tuned = true;
 }
 
-std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s) {
+std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s, int verbose) {
+    PhaseLog log(verbose, "upload", s);
     auto dm = std::make_unique<DeviceModel>();
     const int64_t m = p.A.rows, n = p.A.cols;
     dm->m = static_cast<int>(m);
@@ -174,12 +175,15 @@ std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s) {
     dm->offset = p.objective_offset;
     static const int64_t zero = 0;
     upload_pattern(m, n, m > 0 ? p.A.row_offsets : &zero, p.A.col_indices, dm->a, s);
+    log.mark("pattern (int64 -> int32) + tiles");
     dm->a_val.reset(padded(dm->nnz));
     if (dm->nnz > 0)
         VK_CUDA(cudaMemcpyAsync(dm->a_val.get(), p.A.values, dm->nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+    log.mark("values");
     transpose_pattern(dm->a, dm->at, dm->perm, s);
     dm->at_val.reset(padded(dm->nnz));
     gather_values<double, double>(dm->perm.get(), dm->a_val.get(), dm->at_val.get(), dm->nnz, s);
+    log.mark("transpose");
     if (dm->qp) {
         upload_pattern(n, n, p.Q.row_offsets, p.Q.col_indices, dm->q, s);
         dm->q_val.reset(padded(dm->q_nnz));
@@ -373,7 +377,7 @@ Solver::Solver(const vk_problem &p, const vk_options &o) : opts_(o) {
     device_error_flag(); // allocated here, never inside a graph capture
     VK_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     PhaseLog log(o.verbose, "create", stream_);
-    dm_ = upload_model(p, stream_);
+    dm_ = upload_model(p, stream_, o.verbose);
     log.mark("upload + transpose");
     // the Halpern passes (and the reference scheme's Q pass) run on the
     // patterns' tuned variants; the reference scheme tunes its fused passes itself

@@ -72,7 +72,7 @@ std::string validate_problem(const vk_problem &p, const vk_options &o, bool &uns
 // Uploads a validated problem. The sparse-pass variants of its patterns are
 // timed on first need (ensure_tuned): engines whose passes use the patterns'
 // variants call it; the reference scheme tunes its own two fused passes.
-std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s);
+std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s, int verbose = 0);
 void ensure_tuned(DeviceModel &dm, cudaStream_t s);
 
 // Independent LPs solved together (vk_batch.cu); throws on invalid input.
