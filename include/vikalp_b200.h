@@ -212,6 +212,44 @@ int vk_spmat_variant(const vk_spmat *m, int transpose);
 int vk_spmat_set_variant(vk_spmat *m, int transpose, int variant);
 void vk_spmat_destroy(vk_spmat *m);
 
+/* Replaces the operator's values (nnz doubles, host array, the CSR order it was
+ * created with): ExecutionBackend::set_values (cpu_ops.cpp set_values,
+ * cuda_ops.cu:362-372). Float64 operators only. */
+int vk_spmat_set_values(vk_spmat *m, const double *values, int64_t nnz);
+
+/* ---- device vectors (ExecutionBackend.hpp:36-64) ------------------------------
+ * The vector side of the reference's ExecutionBackend contract, for its CUDA
+ * route (make_cuda_backend, include/vikalp/backend/CudaBackend.hpp in this
+ * repository, built on these). A vk_dvec is n doubles on the device that was
+ * current when it was created; every operation runs on that thread's legacy
+ * default stream, in call order. Semantics are the CPU backend's
+ * (cpu_ops.cpp): axpby rounds alpha*x and beta*y separately (bit-identical to
+ * the CPU loop), project_box is min(max(x, lo), hi) with NaN in x passing
+ * through, norm_inf ignores NaN, dot is a fixed-order tree sum. Size
+ * mismatches return VK_ERR_INVALID naming the operation (the reference throws
+ * std::invalid_argument there). */
+typedef struct vk_dvec vk_dvec;
+int vk_device_select(int32_t device); /* makes `device` current for this thread */
+int vk_device_synchronize(void);     /* waits for the current device's work */
+int vk_dvec_create(int64_t n, vk_dvec **out); /* zero-filled */
+void vk_dvec_destroy(vk_dvec *v);
+int64_t vk_dvec_size(const vk_dvec *v);
+int vk_dvec_upload(vk_dvec *v, const double *host, int64_t n);
+int vk_dvec_download(const vk_dvec *v, double *host, int64_t n); /* returns when the copy is done */
+int vk_dvec_fill(vk_dvec *v, double value);
+int vk_dvec_copy(const vk_dvec *src, vk_dvec *dst);
+int vk_dvec_axpby(double alpha, const vk_dvec *x, double beta, vk_dvec *y); /* y = alpha x + beta y */
+int vk_dvec_dot(const vk_dvec *x, const vk_dvec *y, double *result);
+int vk_dvec_norm_inf(const vk_dvec *x, double *result);
+int vk_dvec_project_box(vk_dvec *x, const vk_dvec *lower, const vk_dvec *upper);
+/* y = alpha * op(A) x + beta * y on device vectors (ExecutionBackend::multiply,
+ * cpu_ops.cpp:393-460, cuda_ops.cu:473-528): x and y distinct, op(A) = A' when
+ * transpose != 0 (the pre-built transposed CSR). VK_SPMV_SEQUENTIAL sums in
+ * the CPU backend's order (bit-identical); VK_SPMV_FAST uses the autotuned
+ * kernels. */
+int vk_spmat_multiply(vk_spmat *m, double alpha, const vk_dvec *x, double beta, vk_dvec *y, int transpose,
+                      int spmv_order);
+
 /* ExecutionBackend::dot and ::norm_inf on device arrays of n doubles
  * (ExecutionBackend.hpp:49-51; cuda_ops.cu:407-451), written to
  * *result_device on `stream` (a cudaStream_t, NULL = default stream). Block

@@ -194,3 +194,17 @@ def test_adjoint_validates_before_the_device():
     with pytest.raises(vk.VkError) as e:
         vk.lp_adjoint([lp], [np.zeros(1)], [np.zeros(1)], [np.ones(1)], solve_tolerance=0.0)
     assert e.value.code == vk.VK_ERR_INVALID
+
+
+def test_device_vector_argument_errors_without_a_gpu():
+    # checked before any CUDA call: a negative size and null handles
+    L = vk.lib()
+    out = C.c_void_p()
+    assert L.vk_dvec_create(-1, C.byref(out)) == vk.VK_ERR_INVALID
+    assert "non-negative" in vk.last_error()
+    assert L.vk_dvec_size(None) == -1
+    r = C.c_double()
+    assert L.vk_dvec_dot(None, None, C.byref(r)) == vk.VK_ERR_INVALID
+    assert L.vk_dvec_axpby(1.0, None, 1.0, None) == vk.VK_ERR_INVALID
+    assert L.vk_spmat_multiply(None, 1.0, None, 0.0, None, 0, 0) == vk.VK_ERR_INVALID
+    assert L.vk_spmat_set_values(None, None, 0) == vk.VK_ERR_INVALID

@@ -109,6 +109,21 @@ _SIGNATURES = {
     "vk_spmat_variant": (C.c_int, [C.c_void_p, C.c_int]),
     "vk_spmat_set_variant": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "vk_spmat_destroy": (None, [C.c_void_p]),
+    "vk_spmat_set_values": (C.c_int, [C.c_void_p, _f64p, C.c_int64]),
+    "vk_spmat_multiply": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_void_p, C.c_int, C.c_int]),
+    "vk_device_select": (C.c_int, [C.c_int32]),
+    "vk_device_synchronize": (C.c_int, []),
+    "vk_dvec_create": (C.c_int, [C.c_int64, C.POINTER(C.c_void_p)]),
+    "vk_dvec_destroy": (None, [C.c_void_p]),
+    "vk_dvec_size": (C.c_int64, [C.c_void_p]),
+    "vk_dvec_upload": (C.c_int, [C.c_void_p, _f64p, C.c_int64]),
+    "vk_dvec_download": (C.c_int, [C.c_void_p, _f64p, C.c_int64]),
+    "vk_dvec_fill": (C.c_int, [C.c_void_p, C.c_double]),
+    "vk_dvec_copy": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "vk_dvec_axpby": (C.c_int, [C.c_double, C.c_void_p, C.c_double, C.c_void_p]),
+    "vk_dvec_dot": (C.c_int, [C.c_void_p, C.c_void_p, _f64p]),
+    "vk_dvec_norm_inf": (C.c_int, [C.c_void_p, _f64p]),
+    "vk_dvec_project_box": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "vk_vec_dot_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "vk_vec_norm_inf_device": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "vk_vec_dot_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),

@@ -330,6 +330,62 @@ int vk_spmat_apply_device(vk_spmat *m, const void *x, void *y, int transpose, vo
     });
 }
 
+int vk_spmat_set_values(vk_spmat *m, const double *values, int64_t nnz) {
+    return guarded([&] {
+        if (!m || (nnz > 0 && !values)) return set_error(VK_ERR_INVALID, "null argument");
+        if (nnz != m->a.nnz)
+            return set_error(VK_ERR_INVALID, "set_values: values size " + std::to_string(nnz) + " != nnz " +
+                                                 std::to_string(m->a.nnz));
+        if (m->precision != VK_PREC_FP64) return set_error(VK_ERR_UNSUPPORTED, "set_values needs a float64 operator");
+        if (nnz > 0) {
+            VK_CUDA(cudaMemcpyAsync(m->v64.get(), values, nnz * sizeof(double), cudaMemcpyHostToDevice, nullptr));
+            vk::gather_values<double, double>(m->perm.get(), m->v64.get(), m->vt64.get(), nnz, nullptr);
+        }
+        return VK_OK;
+    });
+}
+
+int vk_spmat_multiply(vk_spmat *m, double alpha, const vk_dvec *x, double beta, vk_dvec *y, int transpose,
+                      int spmv_order) {
+    return guarded([&] {
+        if (!m || !x || !y) return set_error(VK_ERR_INVALID, "null argument");
+        if (m->precision != VK_PREC_FP64) return set_error(VK_ERR_UNSUPPORTED, "multiply needs a float64 operator");
+        const vk::CsrPattern32 &p = transpose ? m->at : m->a; // p.rows = length of y, p.cols = length of x
+        const char *op = transpose ? "multiply (Yes)" : "multiply (No)";
+        if (vk::dvec_size(x) != p.cols)
+            return set_error(VK_ERR_INVALID, std::string(op) + ": x size " + std::to_string(vk::dvec_size(x)) +
+                                                 " != " + std::to_string(p.cols));
+        if (vk::dvec_size(y) != p.rows)
+            return set_error(VK_ERR_INVALID, std::string(op) + ": y size " + std::to_string(vk::dvec_size(y)) +
+                                                 " != " + std::to_string(p.rows));
+        const bool exact = spmv_order == VK_SPMV_SEQUENTIAL;
+        const double *dx = vk::dvec_ptr(x);
+        double *dy = vk::dvec_ptr(y);
+        if (!transpose) {
+            AxpbyEpi e;
+            e.alpha = alpha;
+            e.beta = beta;
+            e.y = dy;
+            auto M = vk::view(p, m->v64.get());
+            if (exact)
+                vk::launch_tiles<double, double, 1, true>(M, vk::Gathers<double, 1>{{dx}}, e, nullptr);
+            else
+                vk::launch_tiles<double, double, 1, false>(M, vk::Gathers<double, 1>{{dx}}, e, nullptr);
+        } else {
+            ScatterEpi e;
+            e.alpha = alpha;
+            e.beta = beta;
+            e.y = dy;
+            auto M = vk::view(p, m->vt64.get());
+            if (exact)
+                vk::launch_tiles<double, double, 1, true>(M, vk::Gathers<double, 1>{{dx}}, e, nullptr);
+            else
+                vk::launch_tiles<double, double, 1, false>(M, vk::Gathers<double, 1>{{dx}}, e, nullptr);
+        }
+        return VK_OK;
+    });
+}
+
 int64_t vk_spmat_bytes(const vk_spmat *m, int transpose) {
     if (!m) return 0;
     const vk::CsrPattern32 &p = transpose ? m->at : m->a;

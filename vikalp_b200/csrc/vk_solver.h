@@ -64,6 +64,11 @@ private:
     std::unique_ptr<Engine> engine_;
 };
 
+// Device vectors of the ExecutionBackend primitives (vk_backend.cu).
+double *dvec_ptr(vk_dvec *v);
+const double *dvec_ptr(const vk_dvec *v);
+int64_t dvec_size(const vk_dvec *v);
+
 // Validation of a vk_problem with the reference's rules and messages.
 // Returns "" when valid. `unsupported` is set when the failure maps to
 // SolveStatus::UnsupportedModel instead of InvalidModel.
