@@ -210,9 +210,53 @@ class Reference:
         lib.vkref_multiply.restype = C.c_int
         lib.vkref_multiply.argtypes = [C.c_int64, C.c_int64, _i64p, _i64p, _f64p, C.c_double, _f64p,
                                        C.c_int64, C.c_double, _f64p, C.c_int64, C.c_int, C.c_char_p, C.c_int]
+        lib.vkref_mps_read.restype = C.c_void_p
+        lib.vkref_mps_read.argtypes = [C.c_char_p]
+        lib.vkref_mps_ok.argtypes = [C.c_void_p]
+        lib.vkref_mps_sizes.argtypes = [C.c_void_p, _i64p, _i64p, _i64p]
+        lib.vkref_mps_sizes.restype = None
+        lib.vkref_mps_arrays.argtypes = [C.c_void_p, _i64p, _i64p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p,
+                                         C.POINTER(C.c_int32)]
+        lib.vkref_mps_arrays.restype = None
+        lib.vkref_mps_name.restype = C.c_char_p
+        lib.vkref_mps_name.argtypes = [C.c_void_p]
+        lib.vkref_mps_error_count.argtypes = [C.c_void_p]
+        lib.vkref_mps_error.restype = C.c_char_p
+        lib.vkref_mps_error.argtypes = [C.c_void_p, C.c_int, _i64p]
+        lib.vkref_mps_free.argtypes = [C.c_void_p]
+        lib.vkref_mps_free.restype = None
         lib.vkref_pdhg_replay.restype = C.c_double
         lib.vkref_pdhg_replay.argtypes = [C.POINTER(_RefProblem), C.c_double, C.c_int64, _f64p, _f64p]
         self.lib = lib
+
+    def read_mps(self, path):
+        """vikalp::MpsReader::read on `path`: ok flag, errors [(line, message)],
+        and the model's arrays (MpsReader.cpp:10-559)."""
+        h = self.lib.vkref_mps_read(path.encode())
+        try:
+            errors = []
+            for i in range(self.lib.vkref_mps_error_count(h)):
+                ln = C.c_int64()
+                msg = self.lib.vkref_mps_error(h, i, C.byref(ln)).decode()
+                errors.append((int(ln.value), msg))
+            out = {"ok": bool(self.lib.vkref_mps_ok(h)), "errors": errors,
+                   "name": self.lib.vkref_mps_name(h).decode()}
+            m, n, nnz = C.c_int64(), C.c_int64(), C.c_int64()
+            self.lib.vkref_mps_sizes(h, C.byref(m), C.byref(n), C.byref(nnz))
+            m, n, nnz = m.value, n.value, nnz.value
+            ro = np.zeros(m + 1, np.int64)
+            ci = np.zeros(nnz, np.int64)
+            arr = {k: np.zeros(n) for k in ("c", "var_lower", "var_upper")}
+            arr.update(values=np.zeros(nnz), row_lower=np.zeros(m), row_upper=np.zeros(m))
+            types = np.zeros(n, np.int32)
+            if len(out["errors"]) == 0 or out["ok"]:
+                self.lib.vkref_mps_arrays(h, _p(ro, _i64p), _p(ci, _i64p), _p(arr["values"]), _p(arr["c"]),
+                                          _p(arr["var_lower"]), _p(arr["var_upper"]), _p(arr["row_lower"]),
+                                          _p(arr["row_upper"]), types.ctypes.data_as(C.POINTER(C.c_int32)))
+            out.update(m=m, n=n, row_offsets=ro, col_idx=ci, types=types, **arr)
+            return out
+        finally:
+            self.lib.vkref_mps_free(h)
 
     def _prob(self, inst, keep, lower=None, upper=None):
         st = _RefProblem()

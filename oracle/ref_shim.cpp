@@ -11,6 +11,8 @@
 //   vkref_solve                     -> vikalp::solve(Model, SolverOptions) (Solver.hpp:19-21)
 //   vkref_multiply                  -> ExecutionBackend::multiply on the CPU backend
 //                                      (cpu_ops.cpp:393-460)
+//   vkref_mps_*                     -> vikalp::MpsReader::read (src/io/MpsReader.cpp:10-559),
+//                                      the model and errors copied out
 //   vkref_pdhg_replay               -> the per-iteration ExecutionBackend call sequence of
 //                                      pdhg.cpp:92-130 on already-scaled data, for sizes where
 //                                      the reference's own setup cannot finish (its column
@@ -20,6 +22,7 @@
 #include "vikalp/contracts/Model.hpp"
 #include "vikalp/contracts/SolveResult.hpp"
 #include "vikalp/contracts/SolverOptions.hpp"
+#include "vikalp/io/MpsReader.hpp"
 #include "vikalp/solver/Solver.hpp"
 #include "vikalp/solver/continuous.hpp"
 
@@ -263,5 +266,52 @@ double vkref_pdhg_replay(const vkref_problem *p, double step, int64_t iterations
     if (y_out) be->download(*y, std::span<double>(y_out, static_cast<std::size_t>(m)));
     return secs + 0.0 * sink;
 }
+
+struct vkref_mps {
+    vikalp::Model model;
+    std::vector<vikalp::MpsError> errors;
+    int ok = 0;
+};
+
+vkref_mps *vkref_mps_read(const char *path) {
+    auto *h = new vkref_mps();
+    vikalp::MpsReader r;
+    h->ok = r.read(path, h->model) ? 1 : 0;
+    h->errors = r.errors();
+    return h;
+}
+
+int vkref_mps_ok(const vkref_mps *h) { return h->ok; }
+
+void vkref_mps_sizes(const vkref_mps *h, int64_t *m, int64_t *n, int64_t *nnz) {
+    const auto &A = h->model.constraint_matrix;
+    *m = A.pattern.rows;
+    *n = A.pattern.columns;
+    *nnz = static_cast<int64_t>(A.pattern.column_indices.size());
+}
+
+// Arrays sized by vkref_mps_sizes: ro[m+1], ci[nnz], v[nnz], c/vl/vu/types[n], rl/ru[m].
+void vkref_mps_arrays(const vkref_mps *h, int64_t *ro, int64_t *ci, double *v, double *c, double *vl, double *vu,
+                      double *rl, double *ru, int32_t *types) {
+    const vikalp::Model &md = h->model;
+    const auto &A = md.constraint_matrix;
+    std::copy(A.pattern.row_offsets.begin(), A.pattern.row_offsets.end(), ro);
+    std::copy(A.pattern.column_indices.begin(), A.pattern.column_indices.end(), ci);
+    std::copy(A.values.begin(), A.values.end(), v);
+    std::copy(md.linear_objective.begin(), md.linear_objective.end(), c);
+    std::copy(md.variable_lower.begin(), md.variable_lower.end(), vl);
+    std::copy(md.variable_upper.begin(), md.variable_upper.end(), vu);
+    std::copy(md.constraint_lower.begin(), md.constraint_lower.end(), rl);
+    std::copy(md.constraint_upper.begin(), md.constraint_upper.end(), ru);
+    for (std::size_t j = 0; j < md.variable_types.size(); ++j) types[j] = static_cast<int32_t>(md.variable_types[j]);
+}
+
+const char *vkref_mps_name(const vkref_mps *h) { return h->model.name.c_str(); }
+int vkref_mps_error_count(const vkref_mps *h) { return static_cast<int>(h->errors.size()); }
+const char *vkref_mps_error(const vkref_mps *h, int i, int64_t *line) {
+    *line = static_cast<int64_t>(h->errors[static_cast<std::size_t>(i)].line);
+    return h->errors[static_cast<std::size_t>(i)].message.c_str();
+}
+void vkref_mps_free(vkref_mps *h) { delete h; }
 
 } // extern "C"

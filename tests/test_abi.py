@@ -17,9 +17,9 @@ import vikalp_b200 as vk
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_functions():
+def declared_functions(header="vikalp_b200.h"):
     names = set()
-    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+    for h in [os.path.join(ROOT, "include", header)]:
         src = open(h).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(vk_\w+)\s*\(", src, flags=re.M):
@@ -35,6 +35,15 @@ def test_exports_every_declared_symbol():
     assert not missing, missing
     # and the Python binding knows every one of them
     assert names <= set(vk._SIGNATURES), names - set(vk._SIGNATURES)
+    # the MPS entry points live in the C++ host layer
+    mps = declared_functions("vikalp_mps.h")
+    assert {"vk_mps_read", "vk_mps_problem", "vk_mps_free"} <= mps
+    H = C.CDLL(vk.HOST_LIB_PATH)
+    assert not [n for n in sorted(mps) if not hasattr(H, n)]
+    assert mps <= set(vk._MPS_SIGNATURES), mps - set(vk._MPS_SIGNATURES)
+    # every header under include/ is one of the two
+    assert sorted(os.path.basename(h) for h in glob.glob(os.path.join(ROOT, "include", "*.h"))) == \
+        ["vikalp_b200.h", "vikalp_mps.h"]
 
 
 def test_defaults_mirror_solver_options():

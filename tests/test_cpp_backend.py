@@ -19,7 +19,7 @@ def test_binary():
     os.makedirs(BIN_DIR, exist_ok=True)
     exe = os.path.join(BIN_DIR, "test_backend")
     src = os.path.join(ROOT, "tests", "cpp", "test_backend.cpp")
-    cmd = ["g++", "-std=c++20", "-O1", "-I", os.path.join(ROOT, "include"), src, "-L", PKG, "-lvikalp",
+    cmd = [build.CXX, "-std=c++20", "-O1", "-I", os.path.join(ROOT, "include"), src, "-L", PKG, "-lvikalp",
            "-lvikalp_b200", f"-Wl,-rpath,{PKG}", "-o", exe]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr

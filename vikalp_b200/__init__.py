@@ -135,7 +135,88 @@ _SIGNATURES = {
                                 C.POINTER(AdjointOptions), _f64p, _f64p, _f64p, C.POINTER(AdjointInfo)]),
 }
 
+# include/vikalp_mps.h: the MPS ingest path, exported by the C++ host layer (libvikalp.so).
+HOST_LIB_PATH = os.path.join(HERE, "libvikalp.so")
+_MPS_SIGNATURES = {
+    "vk_mps_read": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "vk_mps_problem": (C.c_int, [C.c_void_p, C.POINTER(Problem), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                 C.POINTER(C.c_int64)]),
+    "vk_mps_name": (C.c_char_p, [C.c_void_p]),
+    "vk_mps_binary_count": (C.c_int32, [C.c_void_p]),
+    "vk_mps_error_count": (C.c_int32, [C.c_void_p]),
+    "vk_mps_error": (C.c_char_p, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64)]),
+    "vk_mps_free": (None, [C.c_void_p]),
+}
+
 _lib = None
+_host = None
+
+
+def host_lib():
+    """Loads libvikalp.so, the C++ host layer (raises if it has not been built)."""
+    global _host
+    if _host is None:
+        lib()  # the CUDA library it links against
+        if not os.path.exists(HOST_LIB_PATH):
+            raise ImportError(f"{HOST_LIB_PATH} is missing: build it with `python -m vikalp_b200.build`")
+        L = C.CDLL(HOST_LIB_PATH)
+        for name, (res, args) in _MPS_SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _host = L
+    return _host
+
+
+class MpsModel:
+    """A model read from an MPS file by vikalp::MpsReader (vk_mps_read): the
+    arrays of a synthetic.Instance-like object, plus the reader's errors."""
+
+    def __init__(self, path: str):
+        L = host_lib()
+        h = C.c_void_p()
+        rc = L.vk_mps_read(os.fsencode(path), C.byref(h))
+        if rc == VK_ERR_INTERNAL or not h:
+            raise VkError(rc, "MPS reader failed")
+        try:
+            self.ok = rc == VK_OK
+            self.errors = []
+            for i in range(L.vk_mps_error_count(h)):
+                ln = C.c_int64()
+                msg = L.vk_mps_error(h, i, C.byref(ln)).decode()
+                self.errors.append((int(ln.value), msg))
+            self.name = L.vk_mps_name(h).decode()
+            self.binaries = int(L.vk_mps_binary_count(h))
+            p = Problem()
+            m, n, nnz = C.c_int64(), C.c_int64(), C.c_int64()
+            L.vk_mps_problem(h, C.byref(p), C.byref(m), C.byref(n), C.byref(nnz))
+            self.m, self.n = int(m.value), int(n.value)
+            k = int(nnz.value)
+            cp = lambda ptr, cnt, dt: np.ctypeslib.as_array(ptr, shape=(cnt,)).astype(dt, copy=True) if cnt > 0 else np.zeros(0, dt)  # noqa: E731
+            self.row_offsets = cp(p.A.row_offsets, self.m + 1, np.int64)
+            self.col_idx = cp(p.A.col_indices, k, np.int64)
+            self.values = cp(p.A.values, k, np.float64)
+            self.c = cp(p.c, self.n, np.float64)
+            self.var_lower = cp(p.var_lower, self.n, np.float64)
+            self.var_upper = cp(p.var_upper, self.n, np.float64)
+            self.row_lower = cp(p.row_lower, self.m, np.float64)
+            self.row_upper = cp(p.row_upper, self.m, np.float64)
+            self.objective_offset = float(p.objective_offset)
+            self.q_row_offsets = self.q_col_idx = self.q_values = None
+        finally:
+            L.vk_mps_free(h)
+
+    @property
+    def nnz(self):
+        return int(self.col_idx.shape[0])
+
+    @property
+    def q_nnz(self):
+        return 0
+
+
+def read_mps(path: str) -> MpsModel:
+    return MpsModel(path)
 
 
 def lib():

@@ -74,7 +74,11 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False, e
 
 
 HOST_LIB = os.path.join(PKG, "libvikalp.so")
-CXX = os.environ.get("CXX", "g++")
+# The system compiler, whose libstdc++ is the shared one every Python process
+# here already has loaded (through numpy); a toolchain that links libstdc++
+# statically would put a second copy of the C++ runtime (iostreams, locales)
+# into the process.
+CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else os.environ.get("CXX", "g++")
 
 
 def build_host(force: bool = False) -> str:
