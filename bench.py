@@ -25,6 +25,7 @@ replicas, no collective on the path). The same line carries:
                  in batches, errors against the CPU FP64 KKT gradient
   time_to_tol.qp the convex QP (n=5e5, m=2e5), fp64 vs mixed
   roofline       the sparse-pass kernel against measured HBM bandwidth
+  reference_cuda the reference's own CUDA backend (cuSPARSE) on the same GPU
   cpu_baseline   the reference's CPU implementation on this host
 `python bench.py --impl reference` times the reference's own CPU PDHG
 iteration (oracle/_ref, compiled from the reference sources) on the same LP.
@@ -301,6 +302,25 @@ def adjoint_figures(count=256, checked=3):
             "checked_instances": checked}
 
 
+def reference_cuda_rate(inst, iterations=64):
+    """Iterations/s of the same pdhg.cpp:92-130 call sequence on the reference's
+    own CUDA backend (cuda/cuda_ops.cu, cuSPARSE CSR SpMV with int64 indices,
+    built for sm_100a into oracle/_ref/libvkref_cuda.so) on this GPU: the
+    GPU-to-GPU comparison. None when that build is absent."""
+    from oracle.oracle import Oracle, ReferenceCuda
+    try:
+        ref = ReferenceCuda()
+    except (FileNotFoundError, OSError):
+        return None
+    step = 0.99 / max(1.0, Oracle().operator_bound(inst.row_offsets, inst.col_idx, inst.values, inst.n))
+    ref.pdhg_replay_cuda(inst, step, 2)  # warm-up (cuSPARSE handle, workspaces)
+    secs, _, _ = ref.pdhg_replay_cuda(inst, step, iterations)
+    return {"value": round(iterations / secs, 2), "unit": "iter/s", "iterations": iterations,
+            "note": "the reference's own CUDA backend (cuSPARSE CSR ALG1, int64 indices, host-finished "
+                    "norm_inf twice per iteration) replaying the pdhg.cpp:92-130 call sequence on the same "
+                    "LP and GPU; comparison only"}
+
+
 def reference_cpu_rate(inst, budget_s):
     """Iterations/s of the reference's own CPU PDHG iteration (pdhg.cpp:92-130 call
     sequence through its CPU ExecutionBackend), a bounded sample sized by budget_s."""
@@ -438,6 +458,7 @@ def main():
             line["adjoint"] = adjoint_figures()
             line["time_to_tol"]["qp"] = time_to_tolerance(synthetic.workload_qp(), "qp m=2e5 n=5e5 A nnz=3M Q nnz=1.1M",
                                                           400000, time_limit=120)
+        line["reference_cuda"] = reference_cuda_rate(inst)
         if ws == 1:
             rate, n_it, secs = reference_cpu_rate(inst, budget_s=20.0)
             line["cpu_baseline"] = {"value": round(rate, 4), "unit": "iter/s", "cores": 1, "kind": "reference",

@@ -4,9 +4,13 @@
 ``Reference`` wraps ``oracle/_ref/libvkref.so`` (the reference's own CPU sources,
               built by oracle/Makefile where the reference tree is present; the
               built library travels with the repository snapshot).
+``ReferenceCuda`` wraps ``oracle/_ref/libvkref_cuda.so``: the same sources with
+              the reference's CUDA backend (cuda/cuda_ops.cu, cuSPARSE) built
+              for sm_100a, for the GPU-to-GPU comparison in bench.py.
 
-Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
-these; the CUDA library never does.
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's baseline legs (the
+reference's CPU code, and its CUDA backend as a comparison figure) use these;
+the CUDA library never does.
 """
 
 from __future__ import annotations
@@ -19,6 +23,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libvkref.so")
+REF_CUDA_SO = os.path.join(HERE, "_ref", "libvkref_cuda.so")
 
 _i64p = C.POINTER(C.c_int64)
 _f64p = C.POINTER(C.c_double)
@@ -313,4 +318,27 @@ class Reference:
         x = np.zeros(inst.n)
         y = np.zeros(inst.m)
         secs = self.lib.vkref_pdhg_replay(C.byref(prob), step, iterations, _p(x), _p(y))
+        return secs, x, y
+
+
+class ReferenceCuda(Reference):
+    """The reference built with its CUDA backend (cuda/cuda_ops.cu: cuSPARSE
+    SpMV, SIMT vector kernels, host-finished reductions) for sm_100a -- the
+    GPU-to-GPU comparison. Needs a GPU."""
+
+    def __init__(self, path: str = REF_CUDA_SO):
+        super().__init__(path)
+        self.lib.vkref_pdhg_replay_cuda.restype = C.c_double
+        self.lib.vkref_pdhg_replay_cuda.argtypes = [C.POINTER(_RefProblem), C.c_double, C.c_int64, _f64p, _f64p]
+
+    def pdhg_replay_cuda(self, inst, step, iterations):
+        """Seconds for `iterations` iterations of the pdhg.cpp:92-130 call
+        sequence on the reference's CUDA backend, and the final x, y."""
+        keep = _Keep()
+        prob = self._prob(inst, keep)
+        x = np.zeros(inst.n)
+        y = np.zeros(inst.m)
+        secs = self.lib.vkref_pdhg_replay_cuda(C.byref(prob), step, iterations, _p(x), _p(y))
+        if secs < 0:
+            raise RuntimeError("the reference's CUDA backend threw")
         return secs, x, y

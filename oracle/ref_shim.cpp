@@ -11,6 +11,8 @@
 //   vkref_solve                     -> vikalp::solve(Model, SolverOptions) (Solver.hpp:19-21)
 //   vkref_multiply                  -> ExecutionBackend::multiply on the CPU backend
 //                                      (cpu_ops.cpp:393-460)
+//   vkref_pdhg_replay_cuda          -> the same sequence on the reference's CUDA backend
+//                                      (cuda/cuda_ops.cu), built into _ref/libvkref_cuda.so
 //   vkref_mps_*                     -> vikalp::MpsReader::read (src/io/MpsReader.cpp:10-559),
 //                                      the model and errors copied out
 //   vkref_pdhg_replay               -> the per-iteration ExecutionBackend call sequence of
@@ -18,6 +20,9 @@
 //                                      the reference's own setup cannot finish (its column
 //                                      scaling is O(n*nnz), continuous_common.hpp:160-176).
 #include "vikalp/backend/CpuBackend.hpp"
+#ifdef VKREF_CUDA
+#include "vikalp/backend/CudaBackend.hpp"
+#endif
 #include "vikalp/contracts/ExecutionBackend.hpp"
 #include "vikalp/contracts/Model.hpp"
 #include "vikalp/contracts/SolveResult.hpp"
@@ -202,10 +207,14 @@ int vkref_multiply(int64_t m, int64_t n, const int64_t *ro, const int64_t *ci, c
 // Runs `iterations` passes of the pdhg.cpp:92-130 backend-call sequence (fixed
 // tau = sigma = step) on already-scaled data with the reference CPU backend.
 // Returns seconds spent in the loop; x[n] and y[m] hold the final iterates.
-double vkref_pdhg_replay(const vkref_problem *p, double step, int64_t iterations, double *x_out,
-                         double *y_out) {
+} // extern "C"
+
+namespace {
+// The pdhg.cpp:92-130 call sequence on `bk`; seconds for `iterations` iterations.
+double replay(vikalp::ExecutionBackend &bk, const vkref_problem *p, double step, int64_t iterations, double *x_out,
+              double *y_out) {
     using vikalp::Transpose;
-    auto be = vikalp::make_cpu_backend();
+    vikalp::ExecutionBackend *be = &bk;
     const int64_t m = p->m, n = p->n;
     vikalp::CsrPattern pat;
     pat.rows = m;
@@ -261,11 +270,36 @@ double vkref_pdhg_replay(const vkref_problem *p, double step, int64_t iterations
         be->axpby(-1.0, *px, 1.0, *res);
         sink += be->norm_inf(*res);
     }
+    be->synchronize();
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (x_out) be->download(*x, std::span<double>(x_out, static_cast<std::size_t>(n)));
     if (y_out) be->download(*y, std::span<double>(y_out, static_cast<std::size_t>(m)));
     return secs + 0.0 * sink;
 }
+} // namespace
+
+extern "C" {
+
+double vkref_pdhg_replay(const vkref_problem *p, double step, int64_t iterations, double *x_out,
+                         double *y_out) {
+    auto be = vikalp::make_cpu_backend();
+    return replay(*be, p, step, iterations, x_out, y_out);
+}
+
+#ifdef VKREF_CUDA
+// The same sequence on the reference's CUDA backend (cuda/cuda_ops.cu:
+// cuSPARSE SpMV, SIMT vector kernels, host-finished reductions), for the
+// GPU-to-GPU comparison. Returns -1 when the backend throws.
+double vkref_pdhg_replay_cuda(const vkref_problem *p, double step, int64_t iterations, double *x_out,
+                              double *y_out) {
+    try {
+        auto be = vikalp::make_cuda_backend();
+        return replay(*be, p, step, iterations, x_out, y_out);
+    } catch (const std::exception &) {
+        return -1.0;
+    }
+}
+#endif
 
 struct vkref_mps {
     vikalp::Model model;

@@ -114,6 +114,23 @@ def test_pass_profile(order):
         assert e.value.code == vk.VK_ERR_UNSUPPORTED
 
 
+def test_reference_cuda_backend_runs_on_b200(oracle):
+    # the reference's own CUDA backend (cuSPARSE; the bench's GPU-to-GPU
+    # comparison) replays the reference iteration on this GPU with the same
+    # iterates as its CPU backend, to rounding
+    from oracle.oracle import Reference, ReferenceCuda
+    try:
+        cuda = ReferenceCuda()
+    except (FileNotFoundError, OSError) as e:
+        pytest.skip(f"reference CUDA build absent: {e}")
+    inst = synthetic.lp_uniform(300, 800, 5, seed=3)
+    step = 0.99 / max(1.0, oracle.operator_bound(inst.row_offsets, inst.col_idx, inst.values, inst.n))
+    _, xc, yc = Reference().pdhg_replay(inst, step, 40)
+    _, xg, yg = cuda.pdhg_replay_cuda(inst, step, 40)
+    assert np.max(np.abs(xg - xc)) <= 1e-9 * (1 + np.abs(xc).max())
+    assert np.max(np.abs(yg - yc)) <= 1e-9 * (1 + np.abs(yc).max())
+
+
 def test_repeated_solves_on_one_handle(golden_cases):
     # one device model, several solves with different overrides (the
     # branch-and-bound pattern, RelaxationOracle.hpp:17-22)
