@@ -106,36 +106,6 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def dist_setup(n_gpus):
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if ws > 1:
-        import datetime
-
-        import torch.distributed as dist
-        import torch
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-    return ws, rank, local, dist
-
-
-def barrier(dist):
-    if dist is not None:
-        dist.barrier()
-
-
-def allmax(dist, v, local):
-    if dist is None:
-        return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
 def profile_traffic(kernel_name):
     """DRAM bytes per launch of a fused pass (the column or the row pass of the
     reference-scheme iteration on the large LP) from its committed ncu summary."""
@@ -355,14 +325,16 @@ def main():
     if args.profile_iter:
         return profile_iterations(args.profile_iter)
     K, W = max(1, args.steps), max(3, args.warmup)
-    ws, rank, local, dist = dist_setup(args.gpus)
+    from vikalp_b200 import replicas
     from vikalp_b200 import synthetic
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
     config = {"workload": "lp m=1,000,000 n=2,000,000 nnz~21.1M (Zipf 1.5 column degrees, |a| in 1e-3..1e3)",
               "step": f"{CHUNK} PDHG iterations", "inputs_vs_l2": "inputs larger than L2 (~0.6 GB of matrix per iteration)",
               "parallelism": f"replicas x{ws}"}
 
     if args.impl == "reference":
-        if rank != 0:
+        # rank 0 alone times the reference's CPU code; no process group
+        if int(os.environ.get("RANK", "0")) != 0:
             return 0
         inst = synthetic.workload_large_lp(seed=12345)
         cores = 1
@@ -378,6 +350,8 @@ def main():
         print(json.dumps(line))
         return 0
 
+    ranks = replicas.init()
+    ws, rank, local = ranks.world, ranks.rank, ranks.local
     import torch
 
     import vikalp_b200 as vk
@@ -387,20 +361,19 @@ def main():
     # ---- value: resident data, reference scheme -------------------------------
     h = vk.Pdhg(inst, algorithm="reference", check_every=CHUNK)
     # warm-up: W steps
-    barrier(dist)
+    replicas.barrier(ranks)
     torch.cuda.synchronize()
     _ = solve_with_limit(h, W * CHUNK)
-    barrier(dist)
+    replicas.barrier(ranks)
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        barrier(dist)
+        replicas.barrier(ranks)
         torch.cuda.synchronize()
         r = solve_with_limit(h, K * CHUNK)
         torch.cuda.synchronize()
-        barrier(dist)
-    t_dev = allmax(dist, r["iterate_seconds"], local)
+        replicas.barrier(ranks)
     iters = r["iterations"]
-    value = ws * iters / t_dev
+    value, t_dev = replicas.whole_job_rate(ranks, iters, r["iterate_seconds"])
     ms_per_step = t_dev / (iters / CHUNK) * 1e3
     launches = r["kernel_launches"]
     # per-kernel device times of the same passes on the same handle (eager
@@ -408,16 +381,16 @@ def main():
     prof = h.profile(2 * CHUNK) if rank == 0 else None
     h.close()
     # ---- e2e: through the C ABI from host arrays ---------------------------------
-    barrier(dist)
+    replicas.barrier(ranks)
     t0 = time.perf_counter()
     r2 = vk.solve(inst, algorithm="reference", iteration_limit=K * CHUNK, primal_tolerance=0.0, dual_tolerance=0.0)
     torch.cuda.synchronize()
-    t_e2e = allmax(dist, time.perf_counter() - t0, local)
+    e2e_rate, t_e2e = replicas.whole_job_rate(ranks, r2["iterations"], time.perf_counter() - t0)
     h2d = (inst.row_offsets.nbytes + inst.col_idx.nbytes + inst.values.nbytes + inst.c.nbytes +
            inst.var_lower.nbytes + inst.var_upper.nbytes + inst.row_lower.nbytes + inst.row_upper.nbytes)
     d2h = 8 * (3 * inst.n + 3 * inst.m)  # x, variable duals; y, row duals
     steps_e2e = max(1, r2["iterations"] // CHUNK)
-    e2e = {"value": round(ws * r2["iterations"] / t_e2e, 3), "unit": "iter/s",
+    e2e = {"value": round(e2e_rate, 3), "unit": "iter/s",
            "h2d_bytes_per_step": int(h2d / steps_e2e), "d2h_bytes_per_step": int(d2h / steps_e2e),
            "seconds": round(t_e2e, 3), "note": "create (upload + device setup) + solve + results, pageable host arrays"}
     line = {"metric": METRIC, "value": round(value, 3), "unit": "iter/s", "n_gpus": ws, "steps": iters // CHUNK,
@@ -466,9 +439,7 @@ def main():
                                               f"(its CPU ExecutionBackend) on the large LP, {secs:.1f} s"}
     if rank == 0:
         print(json.dumps(line))
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(ranks)
     return 0
 
 
