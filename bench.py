@@ -381,18 +381,26 @@ def main():
     prof = h.profile(2 * CHUNK) if rank == 0 else None
     h.close()
     # ---- e2e: through the C ABI from host arrays ---------------------------------
-    replicas.barrier(ranks)
-    t0 = time.perf_counter()
-    r2 = vk.solve(inst, algorithm="reference", iteration_limit=K * CHUNK, primal_tolerance=0.0, dual_tolerance=0.0)
-    torch.cuda.synchronize()
-    e2e_rate, t_e2e = replicas.whole_job_rate(ranks, r2["iterations"], time.perf_counter() - t0)
+    # three calls (each: create with upload and device setup, solve, results
+    # back); the median is reported: the host side (page faults of fresh
+    # result arrays, driver allocations) varies from call to call
+    runs = []
+    for _ in range(3):
+        replicas.barrier(ranks)
+        t0 = time.perf_counter()
+        r2 = vk.solve(inst, algorithm="reference", iteration_limit=K * CHUNK, primal_tolerance=0.0,
+                      dual_tolerance=0.0)
+        torch.cuda.synchronize()
+        runs.append(replicas.whole_job_rate(ranks, r2["iterations"], time.perf_counter() - t0))
+    e2e_rate, t_e2e = sorted(runs)[1]
     h2d = (inst.row_offsets.nbytes + inst.col_idx.nbytes + inst.values.nbytes + inst.c.nbytes +
            inst.var_lower.nbytes + inst.var_upper.nbytes + inst.row_lower.nbytes + inst.row_upper.nbytes)
     d2h = 8 * (3 * inst.n + 3 * inst.m)  # x, variable duals; y, row duals
     steps_e2e = max(1, r2["iterations"] // CHUNK)
     e2e = {"value": round(e2e_rate, 3), "unit": "iter/s",
            "h2d_bytes_per_step": int(h2d / steps_e2e), "d2h_bytes_per_step": int(d2h / steps_e2e),
-           "seconds": round(t_e2e, 3), "note": "create (upload + device setup) + solve + results, pageable host arrays"}
+           "seconds": round(t_e2e, 3), "runs_seconds": [round(t, 3) for _, t in runs],
+           "note": "create (upload + device setup) + solve + results, pageable host arrays; median of 3 calls"}
     line = {"metric": METRIC, "value": round(value, 3), "unit": "iter/s", "n_gpus": ws, "steps": iters // CHUNK,
             "warmup": W, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
