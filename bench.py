@@ -317,6 +317,8 @@ def main():
     ap.add_argument("--profile-spmv", choices=["fp64", "fp32"], default=None,
                     help="only run the sparse-product kernel 5 times on the large LP (for ncu captures)")
     ap.add_argument("--transpose", action="store_true", help="with --profile-spmv: A'y instead of A x")
+    ap.add_argument("--profile-shared", type=int, default=0,
+                    help="only run the 512-node shared-matrix batch for this many iterations (for ncu captures)")
     ap.add_argument("--profile-iter", type=int, default=0,
                     help="only run this many reference-scheme iterations on the large LP (for ncu captures)")
     args = ap.parse_args()
@@ -324,6 +326,8 @@ def main():
         return profile_spmv(args.profile_spmv, args.transpose)
     if args.profile_iter:
         return profile_iterations(args.profile_iter)
+    if args.profile_shared:
+        return profile_shared(args.profile_shared)
     K, W = max(1, args.steps), max(3, args.warmup)
     from vikalp_b200 import replicas
     from vikalp_b200 import synthetic
@@ -462,6 +466,19 @@ def profile_iterations(iterations):
         r = h.solve(iteration_limit=iterations, primal_tolerance=0.0, dual_tolerance=0.0, duals=False)
     torch.cuda.synchronize()
     print(f"ok iterations={r['iterations']} status={r['status']}")
+    return 0
+
+
+def profile_shared(iterations):
+    """The batched workload's node half (512 relaxations of the m=5e4, n=1e5 LP,
+    mixed precision) capped at `iterations`, for ncu captures of its SpMM passes."""
+    import vikalp_b200 as vk
+    from vikalp_b200 import synthetic
+    node_lp = synthetic.lp_uniform(50000, 100000, 6, seed=2025)
+    lo, hi = synthetic.bnb_nodes(node_lp, 512, seed=7)
+    rs = vk.batch_solve_shared(node_lp, 512, lo, hi, precision="mixed", iteration_limit=iterations,
+                               relative_tolerance=1e-6)
+    print(f"ok status={rs[0]['status']} iterations={rs[0]['iterations']}")
     return 0
 
 

@@ -25,6 +25,17 @@
 // SM keeps 48+ warps of loads in flight. Rows longer than kCap are streamed by
 // the whole warp.
 //
+// The FAST order has four kernel families, all with the same epilogue
+// interface; the setup autotuner (autotune_pattern, and the reference engine's
+// per-pass tuning) times every variant on the matrix and keeps the fastest:
+// the segmented-scan warp-tile kernel above (tile_kernel_fast), sub-warps of L
+// lanes per row (tile_kernel_sub), lanes owning short rows with longer rows
+// shared by sub-warps or the warp over cost-balanced row chunks
+// (tile_kernel_hyb, the kernel for power-law transposes), and bulk-copy
+// (TMA) staging of each piece's indices and values into shared memory
+// (tile_kernel_tma). Matrices of power-law and uniform rows alike are bound by
+// the random gathers of x (about one L1TEX tag lookup per gather), not by HBM.
+//
 // SEQUENTIAL order (tile_kernel_exact): one thread per row, left to right with
 // each product rounded on its own -- the reference CPU order
 // (cpu_ops.cpp:418-427, 444-458), so results are bit-identical to it. It is
