@@ -1309,7 +1309,7 @@ struct SpmmMat {
 // slice of X (n * 32 * VEC values) at a time and that slice stays in L2. A
 // group whose instances have all stopped is skipped.
 template <class T, int VEC, class Epi>
-__global__ void __launch_bounds__(kSpmmWarps * 32, 3)
+__global__ void __launch_bounds__(kSpmmWarps * 32, 5)
     spmm_kernel(SpmmMat<T> M, const T *__restrict__ X, int ld, int G, Epi epi, double *__restrict__ partials) {
     constexpr int NR = Epi::NR;
     const int p = blockIdx.x, P = gridDim.x;
@@ -1492,9 +1492,9 @@ public:
         vec32_ = B_ >= 128 ? 4 : 1;
         vec64_ = (B_ >= 64 && ld_ % 64 == 0) ? 2 : 1;
         const int sms = sm_count();
-        // one resident wave of blocks; each walks every instance group
-        P32_ = 4 * sms;
-        P64_ = 4 * sms;
+        // one resident wave of blocks (5 per SM, the launch bound); each walks every instance group
+        P32_ = 5 * sms;
+        P64_ = 5 * sms;
         control_arrays();
         pmax_ = std::max(P32_, P64_);
         partial_.reset(static_cast<size_t>(pmax_) * kSpmmMaxR * ld_);
