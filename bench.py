@@ -385,18 +385,18 @@ def main():
     prof = h.profile(2 * CHUNK) if rank == 0 else None
     h.close()
     # ---- e2e: through the C ABI from host arrays ---------------------------------
-    # three calls (each: create with upload and device setup, solve, results
+    # five calls (each: create with upload and device setup, solve, results
     # back); the median is reported: the host side (page faults of fresh
     # result arrays, driver allocations) varies from call to call
     runs = []
-    for _ in range(3):
+    for _ in range(5):
         replicas.barrier(ranks)
         t0 = time.perf_counter()
         r2 = vk.solve(inst, algorithm="reference", iteration_limit=K * CHUNK, primal_tolerance=0.0,
                       dual_tolerance=0.0)
         torch.cuda.synchronize()
         runs.append(replicas.whole_job_rate(ranks, r2["iterations"], time.perf_counter() - t0))
-    e2e_rate, t_e2e = sorted(runs)[1]
+    e2e_rate, t_e2e = sorted(runs)[len(runs) // 2]
     h2d = (inst.row_offsets.nbytes + inst.col_idx.nbytes + inst.values.nbytes + inst.c.nbytes +
            inst.var_lower.nbytes + inst.var_upper.nbytes + inst.row_lower.nbytes + inst.row_upper.nbytes)
     d2h = 8 * (3 * inst.n + 3 * inst.m)  # x, variable duals; y, row duals
@@ -404,7 +404,7 @@ def main():
     e2e = {"value": round(e2e_rate, 3), "unit": "iter/s",
            "h2d_bytes_per_step": int(h2d / steps_e2e), "d2h_bytes_per_step": int(d2h / steps_e2e),
            "seconds": round(t_e2e, 3), "runs_seconds": [round(t, 3) for _, t in runs],
-           "note": "create (upload + device setup) + solve + results, pageable host arrays; median of 3 calls"}
+           "note": "create (upload + device setup) + solve + results, pageable host arrays; median of 5 calls"}
     line = {"metric": METRIC, "value": round(value, 3), "unit": "iter/s", "n_gpus": ws, "steps": iters // CHUNK,
             "warmup": W, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
@@ -429,6 +429,8 @@ def main():
         hal = {}
         for prec in ("fp64", "mixed"):
             with vk.Pdhg(inst, algorithm="halpern", precision=prec, check_every=CHUNK) as hh:
+                # the first solve tunes the passes and captures the graphs; the second is timed
+                solve_with_limit(hh, 2 * CHUNK, rel_tol=0.0)
                 rr = solve_with_limit(hh, 10 * CHUNK, rel_tol=0.0)
             hal[prec] = {"iter_per_s": round(rr["iterations"] / rr["iterate_seconds"], 2),
                          "iterations": rr["iterations"]}

@@ -151,10 +151,13 @@ struct Gathers {
 //         sub-warps of SUB lanes (or by the whole warp)
 //   STAGE > 0: the staged kernel (tile_kernel_tma) with STAGE shared-memory
 //         stages per warp (HYB, SUB as in the hybrid kernel's row sums)
+//   LATE  hybrid kernel only: the epilogue's per-row inputs are loaded after
+//         the row sums instead of before the gathers, so they hold no
+//         registers across them (for the 32-register, 16-CTA builds)
 struct FastVariant {
-    int u, pipe, minb, sub, hyb, stage = 0;
+    int u, pipe, minb, sub, hyb, stage = 0, late = 0;
 };
-constexpr int kFastVariants = 15;
+constexpr int kFastVariants = 17;
 constexpr int kTuneRounds = 4; // timed rounds per variant in the autotuners
 __host__ __device__ constexpr FastVariant fast_variant(int v) {
     return v == 0   ? FastVariant{4, 1, 12, 0, 0}
@@ -171,7 +174,9 @@ __host__ __device__ constexpr FastVariant fast_variant(int v) {
            : v == 11 ? FastVariant{8, 0, 4, 8, 8, 2}
            : v == 12 ? FastVariant{4, 0, 4, 4, 4, 2}
            : v == 13 ? FastVariant{2, 0, 16, 8, 2}
-                     : FastVariant{4, 0, 16, 4, 1};
+           : v == 14 ? FastVariant{4, 0, 16, 4, 1}
+           : v == 15 ? FastVariant{2, 0, 16, 8, 2, 0, 1}
+                     : FastVariant{2, 0, 16, 4, 1, 0, 1};
 }
 
 template <class T, class A, int NV, class Epi, int U, bool PIPE, int MINB>
@@ -519,14 +524,16 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
 // (more than 4*L*U nonzeros), else 32/L at a time by sub-warps of L lanes
 // (U loads per lane in flight, L-wide shuffle reduction); each sum goes back
 // to the row's own lane by a shuffle, and every lane runs its row's epilogue,
-// so the epilogue's loads and stores are coalesced across the group.
+// so the epilogue's loads and stores are coalesced across the group. With
+// LATE the epilogue's inputs are loaded after the sums (other warps hide that
+// latency at full occupancy) rather than held in registers across the gathers.
 // Work: cost-balanced row ranges (chunks, about kChunkCost nonzeros-plus-4-
 // per-row each) round robin over the persistent grid, or the tile schedule's
 // tiles when the epilogue reduces per tile or skips tiles.
 constexpr int kChunkCost = 1024;
 constexpr int kRowCost = 4;
 
-template <class T, class A, int NV, class Epi, int S, int L, int U, int MINB>
+template <class T, class A, int NV, class Epi, int S, int L, int U, int MINB, bool LATE>
 __global__ void __launch_bounds__(kTileThreads, MINB)
     tile_kernel_hyb(CsrView<T> M, Gathers<T, NV> g, Epi epi) {
     static_assert(L == 2 || L == 4 || L == 8 || L == 16, "sub-warp width");
@@ -552,7 +559,7 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
         const int r = rb + lane;
         const bool valid = r < re;
         Pre pre{};
-        if (valid) pre = epi.load(r);
+        if (!LATE && valid) pre = epi.load(r);
         const int len = b - a;
         A sum[NV];
 #pragma unroll
@@ -650,6 +657,7 @@ __global__ void __launch_bounds__(kTileThreads, MINB)
             for (int i = 0; i < G; ++i) lm &= lm - 1u;
         }
         if (valid) {
+            if constexpr (LATE) pre = epi.load(r);
             A s2[NV];
 #pragma unroll
             for (int q = 0; q < NV; ++q) s2[q] = epi.init(r, q) + sum[q];
@@ -946,7 +954,7 @@ inline int launch_fast(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi &
     if constexpr (fv.stage > 0 && staged_ok)
         kernel = tile_kernel_tma<T, A, NV, Epi, fv.hyb, fv.sub, fv.u, fv.minb>;
     else if constexpr (fv.hyb > 0)
-        kernel = tile_kernel_hyb<T, A, NV, Epi, fv.hyb, fv.sub, fv.u, fv.minb>;
+        kernel = tile_kernel_hyb<T, A, NV, Epi, fv.hyb, fv.sub, fv.u, fv.minb, fv.late != 0>;
     else if constexpr (fv.sub > 0)
         kernel = tile_kernel_sub<T, A, NV, Epi, (fv.sub > 0 ? fv.sub : 32), fv.u, fv.minb>;
     else
@@ -994,6 +1002,8 @@ inline int launch_tiles(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi 
     case 12: return launch_fast<T, A, NV, Epi, 12>(M, g, epi, s);
     case 13: return launch_fast<T, A, NV, Epi, 13>(M, g, epi, s);
     case 14: return launch_fast<T, A, NV, Epi, 14>(M, g, epi, s);
+    case 15: return launch_fast<T, A, NV, Epi, 15>(M, g, epi, s);
+    case 16: return launch_fast<T, A, NV, Epi, 16>(M, g, epi, s);
 
     default: return launch_fast<T, A, NV, Epi, 0>(M, g, epi, s);
     }

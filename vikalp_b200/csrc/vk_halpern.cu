@@ -38,6 +38,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <limits>
 
 namespace vk {
@@ -49,6 +50,7 @@ constexpr int kColCheckSums = 2;       // |x^-x|^2, |x^-x0|^2
 constexpr int kRowCheckSums = 2;       // |y^-y|^2, |y^-y0|^2
 constexpr int kKktRowSums = 3;         // primal res^2, dual-obj rows, row-dual violations^2
 constexpr int kKktColSums = 5;         // dual res^2, dual-obj cols, primal obj, box violation^2, x'Qx
+constexpr int64_t kTunePassesMinNnz = 2000000; // per-pass variant tuning from this many nonzeros
 
 struct HalCtl {
     double eta, omega, tau, sigma;
@@ -497,8 +499,25 @@ public:
 
     void run(const double *d_warm, const double *d_lo, const double *d_hi, double *d_xo, double *d_yo, RunInfo &info,
              std::chrono::steady_clock::time_point started) override {
+        start(d_warm, d_lo, d_hi);
+        if (!tuned_) {
+            // once per model, before the graphs are captured; the passes
+            // overwrite the start, so it is set up again afterwards
+            tuned_ = true;
+            tune_passes(s64_, 0);
+            if (mixed_) {
+                copy_state<float, double>(s64_, s32_);
+                tune_passes(s32_, 1);
+            }
+            start(d_warm, d_lo, d_hi);
+        }
+        run_chunks(d_xo, d_yo, info, started);
+    }
+
+    // The solve's start: scaled bounds and start in float64 (copied into the
+    // float32 state when mixed), zero duals, a fresh control block.
+    void start(const double *d_warm, const double *d_lo, const double *d_hi) {
         const int m = dm_.m, n = dm_.n;
-        // scaled bounds / start in float64, copied into the float32 state when mixed
         prepare_kernel<double><<<grid1d(n), 256, 0, s_>>>(d_warm, d_lo, d_hi, cs_.get(), n, s64_.l.get(),
                                                           s64_.u.get(), s64_.x.get(), s64_.x0.get());
         VK_LAUNCH_CHECK();
@@ -523,6 +542,61 @@ public:
         c.status = VK_STATUS_NOT_SOLVED;
         c.kkt = std::numeric_limits<double>::infinity();
         VK_CUDA(cudaMemcpyAsync(ctl_.get(), &c, sizeof(c), cudaMemcpyHostToDevice, s_));
+    }
+
+    // Times every FAST kernel variant on the two fused iteration passes of
+    // one precision (q: 0 float64, 1 float32) and keeps the fastest for each:
+    // their epilogues set the register pressure, so the plain product's
+    // choice need not carry over. One untimed round, then kTuneRounds rounds
+    // with the variants interleaved; each keeps its best round. Models below
+    // kTunePassesMinNnz keep the plain product's variant: there the tuning
+    // (~350 timed launches, the first of each kernel loading its module)
+    // costs as much as a whole solve.
+    template <class T>
+    void tune_passes(HalState<T> &st, int q) {
+        if (forced_variant() >= 0 || dm_.nnz < kTunePassesMinNnz) return;
+        cudaEvent_t a, b;
+        VK_CUDA(cudaEventCreate(&a));
+        VK_CUDA(cudaEventCreate(&b));
+        for (int pass = 0; pass < (st.m > 0 ? 2 : 1); ++pass) {
+            int &var = pass == 0 ? col_var_[q] : row_var_[q];
+            auto launch = [&](int v) {
+                var = v;
+                if (pass == 0)
+                    col_pass<T, false>(st, 0);
+                else
+                    row_pass<T, false>(st, 0);
+            };
+            float best[kFastVariants];
+            for (int v = 0; v < kFastVariants; ++v) {
+                launch(v);
+                best[v] = 1e30f;
+            }
+            for (int round = 0; round < kTuneRounds; ++round)
+                for (int v = 0; v < kFastVariants; ++v) {
+                    VK_CUDA(cudaEventRecord(a, s_));
+                    launch(v);
+                    VK_CUDA(cudaEventRecord(b, s_));
+                    VK_CUDA(cudaEventSynchronize(b));
+                    float ms = 0.f;
+                    VK_CUDA(cudaEventElapsedTime(&ms, a, b));
+                    best[v] = std::min(best[v], ms);
+                }
+            var = static_cast<int>(std::min_element(best, best + kFastVariants) - best);
+            if (o_.verbose > 0) {
+                std::fprintf(stderr, "[vikalp_b200] halpern %s %s pass variants (best of %d, ms):",
+                             q == 0 ? "float64" : "float32", pass == 0 ? "column" : "row", kTuneRounds);
+                for (int v = 0; v < kFastVariants; ++v) std::fprintf(stderr, " %d:%.4f", v, best[v]);
+                std::fprintf(stderr, " -> %d\n", var);
+            }
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        check_device_error(s_);
+    }
+
+    void run_chunks(double *d_xo, double *d_yo, RunInfo &info, std::chrono::steady_clock::time_point started) {
+        const int m = dm_.m, n = dm_.n;
         cudaEvent_t e0, e1;
         VK_CUDA(cudaEventCreate(&e0));
         VK_CUDA(cudaEventCreate(&e1));
@@ -838,6 +912,14 @@ private:
         launch_tiles<T, T, 1, false>(view(dm_.q, st.q.get()), Gathers<T, 1>{{v}}, e, s_);
     }
 
+    // A pass's matrix view with the variant tuned for it (q: 0 float64, 1 float32).
+    template <class T>
+    CsrView<T> pass_view(const CsrPattern32 &p, const T *val, int tuned) const {
+        CsrView<T> v = view(p, val);
+        if (tuned >= 0) v.variant = tuned;
+        return v;
+    }
+
     template <class T, bool CHECK>
     int col_pass(HalState<T> &st, int it) {
         HalColEpi<T, CHECK> e;
@@ -853,7 +935,8 @@ private:
         e.u = st.u.get();
         e.partials = pc_.get();
         const T *yg = st.m > 0 ? st.y.get() : st.x.get();
-        return launch_tiles<T, T, 1, false>(view(dm_.at, st.kat.get()), Gathers<T, 1>{{yg}}, e, s_);
+        return launch_tiles<T, T, 1, false>(pass_view(dm_.at, st.kat.get(), col_var_[sizeof(T) == 4]),
+                                            Gathers<T, 1>{{yg}}, e, s_);
     }
 
     template <class T, bool CHECK>
@@ -868,7 +951,8 @@ private:
         e.rl = st.rl.get();
         e.ru = st.ru.get();
         e.partials = pr_.get();
-        return launch_tiles<T, T, 1, false>(view(dm_.a, st.ka.get()), Gathers<T, 1>{{st.xbar.get()}}, e, s_);
+        return launch_tiles<T, T, 1, false>(pass_view(dm_.a, st.ka.get(), row_var_[sizeof(T) == 4]),
+                                            Gathers<T, 1>{{st.xbar.get()}}, e, s_);
     }
 
     template <class T>
@@ -913,6 +997,8 @@ private:
     double knorm_ = 0.0, lq_ = 0.0, omega0_ = 1.0, bnorm_ = 0.0, cnorm_ = 0.0;
     cudaGraphExec_t g64_ = nullptr, g32_ = nullptr;
     long long graph_nodes_ = 0, launches_ = 0;
+    bool tuned_ = false;
+    int col_var_[2] = {-1, -1}, row_var_[2] = {-1, -1}; // tuned pass variants [float64, float32]
 };
 
 } // namespace

@@ -33,6 +33,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <limits>
 #include <vector>
 
@@ -701,6 +702,12 @@ private:
                 }
             (pass == 0 ? col_variant_ : row_variant_) =
                 static_cast<int>(std::min_element(best, best + kFastVariants) - best);
+            if (o_.verbose > 0) {
+                std::fprintf(stderr, "[vikalp_b200] %s pass variants (best of %d, ms):", pass == 0 ? "column" : "row",
+                             kTuneRounds);
+                for (int v = 0; v < kFastVariants; ++v) std::fprintf(stderr, " %d:%.4f", v, best[v]);
+                std::fprintf(stderr, " -> %d\n", pass == 0 ? col_variant_ : row_variant_);
+            }
         }
         cudaEventDestroy(a);
         cudaEventDestroy(b);
