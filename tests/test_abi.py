@@ -120,6 +120,28 @@ def test_malformed_csr():
     assert create_error(m)[1] == "constraint matrix coefficients must be finite"
 
 
+def test_malformed_csr_large_first_error_wins():
+    # patterns of more than 2^20 rows are checked on several host threads; the
+    # message is still the one of the first failing row in order
+    rows = 3 << 20
+    ro = np.arange(rows + 1, dtype=np.int64) * 2
+    ci = np.tile(np.array([0, 1], np.int64), rows)
+    m = M(m=rows, n=3, row_offsets=ro, col_idx=ci.copy(), values=np.ones(2 * rows), c=np.zeros(3),
+          var_lower=np.zeros(3), var_upper=np.ones(3), row_lower=np.zeros(rows), row_upper=np.ones(rows))
+    m.col_idx[2 * (rows - 10)] = 7                   # out of range, late
+    m.col_idx[2 * (rows // 2) + 1] = 0              # unordered, earlier
+    assert create_error(m)[1] == "constraint matrix columns must be strictly ordered per row"
+    m.col_idx[2 * 1000] = -1                        # out of range, earliest
+    assert create_error(m)[1] == "constraint matrix contains an out-of-range column"
+    m.col_idx = ci.copy()
+    m.values[2 * rows - 1] = np.nan                 # the last coefficient
+    assert create_error(m)[1] == "constraint matrix coefficients must be finite"
+    m.values[2 * rows - 1] = 1.0
+    m.row_offsets = ro.copy()
+    m.row_offsets[rows - 5] = 2 * rows + 4          # beyond nnz: rows - 6 and rows - 5 fail
+    assert create_error(m)[1] == "constraint matrix row_offsets must be ordered and in range"
+
+
 def test_row_bounds_invalid():
     m = M(m=1, row_offsets=np.array([0, 1]), col_idx=np.array([0]), values=np.array([1.0]),
           row_lower=np.array([2.0]), row_upper=np.array([1.0]))

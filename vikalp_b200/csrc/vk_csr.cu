@@ -341,32 +341,13 @@ void autotune_pattern(CsrPattern32 &p, const T *val, cudaStream_t s, int64_t min
     e.b = pre.get() + p.rows;
     e.lo = pre.get() + 2 * static_cast<size_t>(p.rows);
     e.hi = pre.get() + 3 * static_cast<size_t>(p.rows);
-    cudaEvent_t a, b;
-    VK_CUDA(cudaEventCreate(&a));
-    VK_CUDA(cudaEventCreate(&b));
-    // one untimed round, then the variants interleaved over rounds (clock
-    // drift hits them alike); each keeps its best round
     float best[kFastVariants];
-    for (int v = 0; v < kFastVariants; ++v) {
-        p.variant = v;
-        launch_tiles<T, T, 1, false>(view(p, val), Gathers<T, 1>{{x.get()}}, e, s);
-        best[v] = 1e30f;
-    }
-    for (int round = 0; round < kTuneRounds; ++round)
-        for (int v = 0; v < kFastVariants; ++v) {
+    const int best_v = tune_variants(
+        [&](int v) {
             p.variant = v;
-            const CsrView<T> M = view(p, val);
-            VK_CUDA(cudaEventRecord(a, s));
-            launch_tiles<T, T, 1, false>(M, Gathers<T, 1>{{x.get()}}, e, s);
-            VK_CUDA(cudaEventRecord(b, s));
-            VK_CUDA(cudaEventSynchronize(b));
-            float t = 0.f;
-            VK_CUDA(cudaEventElapsedTime(&t, a, b));
-            best[v] = std::min(best[v], t);
-        }
-    const int best_v = static_cast<int>(std::min_element(best, best + kFastVariants) - best);
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
+            launch_tiles<T, T, 1, false>(view(p, val), Gathers<T, 1>{{x.get()}}, e, s);
+        },
+        s, best);
     p.variant = best_v;
 }
 

@@ -44,6 +44,8 @@
 
 #include "vk_common.cuh"
 
+#include <algorithm>
+
 namespace vk {
 
 constexpr int kWarps = 4;                  // warps per CTA
@@ -158,7 +160,8 @@ struct FastVariant {
     int u, pipe, minb, sub, hyb, stage = 0, late = 0;
 };
 constexpr int kFastVariants = 17;
-constexpr int kTuneRounds = 4; // timed rounds per variant in the autotuners
+constexpr int kTuneRounds = 4;    // timed rounds per variant in the autotuners
+constexpr float kTuneKeep = 1.25f; // variants slower than this x the best leave after the first timed round
 __host__ __device__ constexpr FastVariant fast_variant(int v) {
     return v == 0   ? FastVariant{4, 1, 12, 0, 0}
            : v == 1 ? FastVariant{8, 1, 8, 0, 0}
@@ -970,6 +973,46 @@ inline int launch_fast(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi &
     kernel<<<grid, kTileThreads, smem, s>>>(M, g, epi);
     VK_LAUNCH_CHECK();
     return grid;
+}
+
+// Times launch(v) -- one launch of a pass with FAST variant v on stream s --
+// for every variant and returns the fastest: one untimed round, one timed
+// round over all variants, then kTuneRounds - 1 rounds over those within
+// kTuneKeep of the best. Rounds interleave the variants (clock drift hits
+// them alike) and each variant keeps its best round in best[v] (a dropped
+// variant: its first timed round). A round's launches queue back to back,
+// one event pair each, and the host waits once per round.
+template <class L>
+int tune_variants(L &&launch, cudaStream_t s, float (&best)[kFastVariants]) {
+    cudaEvent_t ev[2 * kFastVariants];
+    for (cudaEvent_t &e : ev) VK_CUDA(cudaEventCreate(&e));
+    bool keep[kFastVariants];
+    for (int v = 0; v < kFastVariants; ++v) {
+        launch(v);
+        best[v] = 1e30f;
+        keep[v] = true;
+    }
+    for (int round = 0; round < kTuneRounds; ++round) {
+        for (int v = 0; v < kFastVariants; ++v) {
+            if (!keep[v]) continue;
+            VK_CUDA(cudaEventRecord(ev[2 * v], s));
+            launch(v);
+            VK_CUDA(cudaEventRecord(ev[2 * v + 1], s));
+        }
+        VK_CUDA(cudaStreamSynchronize(s));
+        float lo = 1e30f;
+        for (int v = 0; v < kFastVariants; ++v) {
+            if (!keep[v]) continue;
+            float ms = 0.f;
+            VK_CUDA(cudaEventElapsedTime(&ms, ev[2 * v], ev[2 * v + 1]));
+            best[v] = std::min(best[v], ms);
+            lo = std::min(lo, best[v]);
+        }
+        if (round == 0)
+            for (int v = 0; v < kFastVariants; ++v) keep[v] = best[v] <= kTuneKeep * lo;
+    }
+    for (cudaEvent_t &e : ev) cudaEventDestroy(e);
+    return static_cast<int>(std::min_element(best, best + kFastVariants) - best);
 }
 
 // Launches the pass; returns the number of CTAs (the entries a per-CTA

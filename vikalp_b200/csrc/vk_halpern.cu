@@ -547,17 +547,14 @@ public:
     // Times every FAST kernel variant on the two fused iteration passes of
     // one precision (q: 0 float64, 1 float32) and keeps the fastest for each:
     // their epilogues set the register pressure, so the plain product's
-    // choice need not carry over. One untimed round, then kTuneRounds rounds
-    // with the variants interleaved; each keeps its best round. Models below
+    // choice need not carry over (tune_variants: interleaved rounds, the
+    // clearly slower variants dropped after the first). Models below
     // kTunePassesMinNnz keep the plain product's variant: there the tuning
-    // (~350 timed launches, the first of each kernel loading its module)
+    // (~150 timed launches, the first of each kernel loading its module)
     // costs as much as a whole solve.
     template <class T>
     void tune_passes(HalState<T> &st, int q) {
         if (forced_variant() >= 0 || dm_.nnz < kTunePassesMinNnz) return;
-        cudaEvent_t a, b;
-        VK_CUDA(cudaEventCreate(&a));
-        VK_CUDA(cudaEventCreate(&b));
         for (int pass = 0; pass < (st.m > 0 ? 2 : 1); ++pass) {
             int &var = pass == 0 ? col_var_[q] : row_var_[q];
             auto launch = [&](int v) {
@@ -568,30 +565,15 @@ public:
                     row_pass<T, false>(st, 0);
             };
             float best[kFastVariants];
-            for (int v = 0; v < kFastVariants; ++v) {
-                launch(v);
-                best[v] = 1e30f;
-            }
-            for (int round = 0; round < kTuneRounds; ++round)
-                for (int v = 0; v < kFastVariants; ++v) {
-                    VK_CUDA(cudaEventRecord(a, s_));
-                    launch(v);
-                    VK_CUDA(cudaEventRecord(b, s_));
-                    VK_CUDA(cudaEventSynchronize(b));
-                    float ms = 0.f;
-                    VK_CUDA(cudaEventElapsedTime(&ms, a, b));
-                    best[v] = std::min(best[v], ms);
-                }
-            var = static_cast<int>(std::min_element(best, best + kFastVariants) - best);
+            const int pick = tune_variants(launch, s_, best);
+            var = pick;
             if (o_.verbose > 0) {
-                std::fprintf(stderr, "[vikalp_b200] halpern %s %s pass variants (best of %d, ms):",
-                             q == 0 ? "float64" : "float32", pass == 0 ? "column" : "row", kTuneRounds);
+                std::fprintf(stderr, "[vikalp_b200] halpern %s %s pass variants (ms, best timed round):",
+                             q == 0 ? "float64" : "float32", pass == 0 ? "column" : "row");
                 for (int v = 0; v < kFastVariants; ++v) std::fprintf(stderr, " %d:%.4f", v, best[v]);
                 std::fprintf(stderr, " -> %d\n", var);
             }
         }
-        cudaEventDestroy(a);
-        cudaEventDestroy(b);
         check_device_error(s_);
     }
 

@@ -6,6 +6,8 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <thread>
+#include <vector>
 
 namespace vk {
 
@@ -16,6 +18,36 @@ namespace vk {
 // ---------------------------------------------------------------------------
 namespace {
 
+// First failing index of [0, count) in order, or -1. check(b, e, &code)
+// returns the first failing index of [b, e) (-1 if none) and its error code.
+// When the scan touches at least 2^20 elements (`work`) the range is split
+// over host threads; the failure of the lowest range wins, so the result is
+// the sequential scan's.
+template <class F>
+int64_t first_failure(int64_t count, int64_t work, F check, int &code) {
+    constexpr int64_t kSerial = int64_t(1) << 20;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int T = work < kSerial || count < 2 ? 1 : static_cast<int>(std::min<unsigned>(hw == 0 ? 1 : hw, 16));
+    if (T <= 1) return check(0, count, code);
+    std::vector<int64_t> at(T, -1);
+    std::vector<int> codes(T, 0);
+    std::vector<std::thread> pool;
+    pool.reserve(T - 1);
+    auto part = [&](int t) {
+        const int64_t b = count * t / T, e = count * (t + 1) / T;
+        at[t] = check(b, e, codes[t]);
+    };
+    for (int t = 1; t < T; ++t) pool.emplace_back(part, t);
+    part(0);
+    for (auto &th : pool) th.join();
+    for (int t = 0; t < T; ++t)
+        if (at[t] >= 0) {
+            code = codes[t];
+            return at[t];
+        }
+    return -1;
+}
+
 std::string check_pattern(const vk_csr &a, const char *name) {
     const std::string nm(name);
     if (a.rows < 0 || a.cols < 0) return nm + " dimensions must be non-negative";
@@ -25,18 +57,37 @@ std::string check_pattern(const vk_csr &a, const char *name) {
     if (ro[0] != 0) return nm + " row_offsets do not describe column_indices";
     const int64_t nnz = ro[a.rows];
     if (nnz < 0) return nm + " row_offsets must be ordered and in range";
-    for (int64_t r = 0; r < a.rows; ++r) {
-        const int64_t b = ro[r], e = ro[r + 1];
-        if (b < 0 || b > e || e > nnz) return nm + " row_offsets must be ordered and in range";
-        int64_t prev = -1;
-        for (int64_t k = b; k < e; ++k) {
-            const int64_t c = a.col_indices[k];
-            if (c < 0 || c >= a.cols) return nm + " contains an out-of-range column";
-            if (c <= prev) return nm + " columns must be strictly ordered per row";
-            prev = c;
+    enum { kRange = 1, kColumn = 2, kOrder = 3 };
+    auto rows = [&](int64_t r0, int64_t r1, int &code) -> int64_t {
+        for (int64_t r = r0; r < r1; ++r) {
+            const int64_t b = ro[r], e = ro[r + 1];
+            if (b < 0 || b > e || e > nnz) {
+                code = kRange;
+                return r;
+            }
+            int64_t prev = -1;
+            for (int64_t k = b; k < e; ++k) {
+                const int64_t c = a.col_indices[k];
+                if (c < 0 || c >= a.cols) {
+                    code = kColumn;
+                    return r;
+                }
+                if (c <= prev) {
+                    code = kOrder;
+                    return r;
+                }
+                prev = c;
+            }
         }
-    }
-    return "";
+        return -1;
+    };
+    // rows are split evenly; a thread's rows can hold many more nonzeros than
+    // another's only for very skewed patterns, which then just run longer
+    int code = 0;
+    if (first_failure(a.rows, a.rows + nnz, rows, code) < 0) return "";
+    return code == kRange    ? nm + " row_offsets must be ordered and in range"
+           : code == kColumn ? nm + " contains an out-of-range column"
+                             : nm + " columns must be strictly ordered per row";
 }
 
 int64_t nnz_of(const vk_csr &a) { return (a.rows >= 0 && a.row_offsets) ? a.row_offsets[a.rows] : 0; }
@@ -44,9 +95,14 @@ int64_t nnz_of(const vk_csr &a) { return (a.rows >= 0 && a.row_offsets) ? a.row_
 std::string check_matrix(const vk_csr &a, const char *name) {
     std::string e = check_pattern(a, name);
     if (!e.empty()) return e;
+    auto finite = [&](int64_t b, int64_t e2, int &) -> int64_t {
+        for (int64_t k = b; k < e2; ++k)
+            if (!std::isfinite(a.values[k])) return k;
+        return -1;
+    };
+    int code = 0;
     const int64_t nnz = nnz_of(a);
-    for (int64_t k = 0; k < nnz; ++k)
-        if (!std::isfinite(a.values[k])) return std::string(name) + " coefficients must be finite";
+    if (first_failure(nnz, nnz, finite, code) >= 0) return std::string(name) + " coefficients must be finite";
     return "";
 }
 

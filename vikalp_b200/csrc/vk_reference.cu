@@ -654,9 +654,6 @@ private:
         }
         if (exact_ || dm_.nnz < 200000 || dm_.m == 0) return;
         prepare(nullptr, dm_.vl.get(), dm_.vu.get(), std::numeric_limits<long long>::max() / 4, 0.0);
-        cudaEvent_t a, b;
-        VK_CUDA(cudaEventCreate(&a));
-        VK_CUDA(cudaEventCreate(&b));
         for (int pass = 0; pass < 2; ++pass) {
             auto launch = [&](int v) {
                 if (pass == 0) {
@@ -683,34 +680,16 @@ private:
                     tiles(row_view(), Gathers<double, 1>{{x_[1].get()}}, r);
                 }
             };
-            // one untimed round, then the variants interleaved over rounds
-            // (clock drift hits them alike); each keeps its best round
             float best[kFastVariants];
-            for (int v = 0; v < kFastVariants; ++v) {
-                launch(v);
-                best[v] = 1e30f;
-            }
-            for (int round = 0; round < kTuneRounds; ++round)
-                for (int v = 0; v < kFastVariants; ++v) {
-                    VK_CUDA(cudaEventRecord(a, s_));
-                    launch(v);
-                    VK_CUDA(cudaEventRecord(b, s_));
-                    VK_CUDA(cudaEventSynchronize(b));
-                    float ms = 0.f;
-                    VK_CUDA(cudaEventElapsedTime(&ms, a, b));
-                    best[v] = std::min(best[v], ms);
-                }
-            (pass == 0 ? col_variant_ : row_variant_) =
-                static_cast<int>(std::min_element(best, best + kFastVariants) - best);
+            const int pick = tune_variants(launch, s_, best);
+            (pass == 0 ? col_variant_ : row_variant_) = pick;
             if (o_.verbose > 0) {
-                std::fprintf(stderr, "[vikalp_b200] %s pass variants (best of %d, ms):", pass == 0 ? "column" : "row",
-                             kTuneRounds);
+                std::fprintf(stderr, "[vikalp_b200] %s pass variants (ms, best timed round):",
+                             pass == 0 ? "column" : "row");
                 for (int v = 0; v < kFastVariants; ++v) std::fprintf(stderr, " %d:%.4f", v, best[v]);
                 std::fprintf(stderr, " -> %d\n", pass == 0 ? col_variant_ : row_variant_);
             }
         }
-        cudaEventDestroy(a);
-        cudaEventDestroy(b);
         check_device_error(s_);
     }
 
