@@ -1,6 +1,7 @@
 // extern "C" entry points of include/vikalp_b200.h. Every call catches and
 // maps exceptions to status codes; the message is kept per thread.
 #include "vk_engine.cuh"
+#include "vk_stage.cuh"
 #include "vk_vec.cuh"
 
 #include <cstring>
@@ -286,7 +287,7 @@ int vk_spmat_create(const vk_csr *a, int32_t precision, vk_spmat **out) {
         const int64_t nnz = h->a.nnz;
         vk::transpose_pattern(h->a, h->at, h->perm, st.s);
         vk::DevBuf<double> v(vk::padded(nnz));
-        if (nnz > 0) VK_CUDA(cudaMemcpyAsync(v.get(), a->values, nnz * sizeof(double), cudaMemcpyHostToDevice, st.s));
+        vk::stage_h2d(v.get(), a->values, nnz * sizeof(double), st.s);
         if (precision == VK_PREC_FP64) {
             h->vt64.reset(vk::padded(nnz));
             vk::gather_values<double, double>(h->perm.get(), v.get(), h->vt64.get(), nnz, st.s);

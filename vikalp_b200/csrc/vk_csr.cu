@@ -1,6 +1,7 @@
 // Device-side CSR setup: int64 -> int32 conversion, tile schedules, stable
 // transpose. All O(nnz) on the GPU.
 #include "vk_csr.cuh"
+#include "vk_stage.cuh"
 
 #include <algorithm>
 #include <cstdlib>
@@ -12,11 +13,6 @@
 namespace vk {
 
 namespace {
-
-__global__ void narrow_kernel(const int64_t *__restrict__ src, int *__restrict__ dst, int64_t n) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        dst[i] = static_cast<int>(src[i]);
-}
 
 // flags[r] = 1 where a tile starts at row r (r == rows marks the end): rows
 // longer than `short_max` alone, others grouped while their starts fall in
@@ -196,20 +192,9 @@ void upload_pattern(int64_t rows, int64_t cols, const int64_t *h_ro, const int64
     out.ro.reset(rows + 1);
     out.ci.reset(padded(nnz));
     VK_CUDA(cudaMemsetAsync(out.ci.get(), 0, padded(nnz) * sizeof(int), s));
-    {
-        DevBuf<int64_t> t(rows + 1);
-        VK_CUDA(cudaMemcpyAsync(t.get(), h_ro, (rows + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
-        narrow_kernel<<<grid_for(rows + 1), 256, 0, s>>>(t.get(), out.ro.get(), rows + 1);
-        VK_LAUNCH_CHECK();
-        VK_CUDA(cudaStreamSynchronize(s));
-    }
-    if (nnz > 0) {
-        DevBuf<int64_t> t(nnz);
-        VK_CUDA(cudaMemcpyAsync(t.get(), h_ci, nnz * sizeof(int64_t), cudaMemcpyHostToDevice, s));
-        narrow_kernel<<<grid_for(nnz), 256, 0, s>>>(t.get(), out.ci.get(), nnz);
-        VK_LAUNCH_CHECK();
-        VK_CUDA(cudaStreamSynchronize(s));
-    }
+    // int64 -> int32 while staging (validated: every offset and index fits)
+    stage_h2d_narrow(out.ro.get(), h_ro, rows + 1, s);
+    stage_h2d_narrow(out.ci.get(), h_ci, nnz, s);
     int mr = 0;
     for (int64_t r = 0; r < rows; ++r) mr = std::max<int>(mr, static_cast<int>(h_ro[r + 1] - h_ro[r]));
     out.max_row = mr;

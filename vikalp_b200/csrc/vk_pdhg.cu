@@ -1,6 +1,7 @@
 // Solver shell: model validation, upload, and the post-processing that turns
 // final iterates into a SolveResult in original coordinates.
 #include "vk_engine.cuh"
+#include "vk_stage.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -233,8 +234,7 @@ std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s, i
     upload_pattern(m, n, m > 0 ? p.A.row_offsets : &zero, p.A.col_indices, dm->a, s);
     log.mark("pattern (int64 -> int32) + tiles");
     dm->a_val.reset(padded(dm->nnz));
-    if (dm->nnz > 0)
-        VK_CUDA(cudaMemcpyAsync(dm->a_val.get(), p.A.values, dm->nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+    stage_h2d(dm->a_val.get(), p.A.values, dm->nnz * sizeof(double), s);
     log.mark("values");
     transpose_pattern(dm->a, dm->at, dm->perm, s);
     dm->at_val.reset(padded(dm->nnz));
@@ -243,14 +243,14 @@ std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s, i
     if (dm->qp) {
         upload_pattern(n, n, p.Q.row_offsets, p.Q.col_indices, dm->q, s);
         dm->q_val.reset(padded(dm->q_nnz));
-        VK_CUDA(cudaMemcpyAsync(dm->q_val.get(), p.Q.values, dm->q_nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+        stage_h2d(dm->q_val.get(), p.Q.values, dm->q_nnz * sizeof(double), s);
         dm->h_qro.assign(p.Q.row_offsets, p.Q.row_offsets + n + 1);
         dm->h_qci.assign(p.Q.col_indices, p.Q.col_indices + dm->q_nnz);
         dm->h_qv.assign(p.Q.values, p.Q.values + dm->q_nnz);
     }
     auto up = [&](DevBuf<double> &b, const double *h, int64_t k) {
         b.reset(k > 0 ? k : 1);
-        if (k > 0) VK_CUDA(cudaMemcpyAsync(b.get(), h, k * sizeof(double), cudaMemcpyHostToDevice, s));
+        if (k > 0) stage_h2d(b.get(), h, k * sizeof(double), s);
     };
     up(dm->c, p.c, n);
     up(dm->vl, p.var_lower, n);
@@ -594,16 +594,12 @@ void Solver::solve(const double *warm, const double *lo_ovr, const double *hi_ov
     VK_CUDA(cudaMemcpyAsync(&hp, post.get(), sizeof(hp), cudaMemcpyDeviceToHost, s));
     VK_CUDA(cudaMemcpyAsync(hs, sums.get(), sizeof(hs), cudaMemcpyDeviceToHost, s));
     std::vector<double> hx(n);
-    VK_CUDA(cudaMemcpyAsync(hx.data(), xo.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (r->y && m > 0) VK_CUDA(cudaMemcpyAsync(r->y, yo.get(), m * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (r->row_lower_dual && m > 0)
-        VK_CUDA(cudaMemcpyAsync(r->row_lower_dual, ld.get(), m * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (r->row_upper_dual && m > 0)
-        VK_CUDA(cudaMemcpyAsync(r->row_upper_dual, ud.get(), m * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (r->var_lower_dual)
-        VK_CUDA(cudaMemcpyAsync(r->var_lower_dual, vld.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (r->var_upper_dual)
-        VK_CUDA(cudaMemcpyAsync(r->var_upper_dual, vud.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    stage_d2h(hx.data(), xo.get(), n * sizeof(double), s);
+    if (r->y && m > 0) stage_d2h(r->y, yo.get(), m * sizeof(double), s);
+    if (r->row_lower_dual && m > 0) stage_d2h(r->row_lower_dual, ld.get(), m * sizeof(double), s);
+    if (r->row_upper_dual && m > 0) stage_d2h(r->row_upper_dual, ud.get(), m * sizeof(double), s);
+    if (r->var_lower_dual) stage_d2h(r->var_lower_dual, vld.get(), n * sizeof(double), s);
+    if (r->var_upper_dual) stage_d2h(r->var_upper_dual, vud.get(), n * sizeof(double), s);
     VK_CUDA(cudaStreamSynchronize(s));
     if (r->x) std::memcpy(r->x, hx.data(), n * sizeof(double));
 

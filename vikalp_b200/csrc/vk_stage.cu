@@ -1,0 +1,148 @@
+// Staged host <-> device copies (vk_stage.cuh).
+#include "vk_stage.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <exception>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+namespace vk {
+namespace {
+
+// Process-wide pool of pinned kStageChunk-byte buffers. Buffers are kept for
+// the life of the process (freeing pinned memory from a static destructor
+// can run after the CUDA runtime has shut down).
+std::mutex g_pool_mu;
+std::vector<void *> g_pool;
+
+void *acquire_pinned() {
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        if (!g_pool.empty()) {
+            void *p = g_pool.back();
+            g_pool.pop_back();
+            return p;
+        }
+    }
+    void *p = nullptr;
+    VK_CUDA(cudaHostAlloc(&p, kStageChunk, cudaHostAllocPortable));
+    return p;
+}
+
+void release_pinned(void *p) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    g_pool.push_back(p);
+}
+
+// Runs body(chunk, buffer, event, pending) for chunks 0..nchunks-1, chunk i on
+// thread i % T, each thread with its own pinned buffer and event; `pending`
+// says the buffer's last DMA may still be running. A thread waits for its
+// last DMA before its buffer goes back to the pool, also after an error; the
+// first error is rethrown on the calling thread.
+template <class Body>
+void run_staged(int64_t nchunks, Body body) {
+    int dev = 0;
+    VK_CUDA(cudaGetDevice(&dev));
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int T = static_cast<int>(std::max<int64_t>(
+        1, std::min<int64_t>({static_cast<int64_t>(kStageThreads), nchunks, static_cast<int64_t>(hw == 0 ? 1 : hw)})));
+    std::vector<std::exception_ptr> errs(T);
+    auto work = [&](int t) {
+        void *buf = nullptr;
+        cudaEvent_t ev = nullptr;
+        bool pending = false;
+        try {
+            VK_CUDA(cudaSetDevice(dev));
+            buf = acquire_pinned();
+            // blocking sync: a waiting thread sleeps instead of spinning on a core
+            VK_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming | cudaEventBlockingSync));
+            for (int64_t i = t; i < nchunks; i += T) body(i, buf, ev, pending);
+            if (pending) VK_CUDA(cudaEventSynchronize(ev));
+            pending = false;
+        } catch (...) {
+            errs[t] = std::current_exception();
+        }
+        if (pending) cudaEventSynchronize(ev);
+        if (ev) cudaEventDestroy(ev);
+        if (buf) release_pinned(buf);
+    };
+    std::vector<std::thread> pool;
+    pool.reserve(T - 1);
+    for (int t = 1; t < T; ++t) pool.emplace_back(work, t);
+    work(0);
+    for (std::thread &th : pool) th.join();
+    for (const std::exception_ptr &e : errs)
+        if (e) std::rethrow_exception(e);
+}
+
+} // namespace
+
+void stage_h2d(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+    if (bytes == 0) return;
+    if (bytes < kStageMin) {
+        VK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+        VK_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    char *d = static_cast<char *>(dst);
+    const char *h = static_cast<const char *>(src);
+    const int64_t nchunks = static_cast<int64_t>((bytes + kStageChunk - 1) / kStageChunk);
+    run_staged(nchunks, [&](int64_t i, void *buf, cudaEvent_t ev, bool &pending) {
+        const size_t off = static_cast<size_t>(i) * kStageChunk;
+        const size_t n = std::min(kStageChunk, bytes - off);
+        if (pending) VK_CUDA(cudaEventSynchronize(ev));
+        std::memcpy(buf, h + off, n);
+        VK_CUDA(cudaMemcpyAsync(d + off, buf, n, cudaMemcpyHostToDevice, s));
+        VK_CUDA(cudaEventRecord(ev, s));
+        pending = true;
+    });
+}
+
+void stage_h2d_narrow(int *dst, const int64_t *src, int64_t count, cudaStream_t s) {
+    if (count <= 0) return;
+    constexpr int64_t kPer = static_cast<int64_t>(kStageChunk / sizeof(int)); // int32 outputs per chunk
+    if (static_cast<size_t>(count) * sizeof(int64_t) < kStageMin) {
+        std::vector<int> tmp(static_cast<size_t>(count));
+        for (int64_t i = 0; i < count; ++i) tmp[static_cast<size_t>(i)] = static_cast<int>(src[i]);
+        VK_CUDA(cudaMemcpyAsync(dst, tmp.data(), count * sizeof(int), cudaMemcpyHostToDevice, s));
+        VK_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    const int64_t nchunks = (count + kPer - 1) / kPer;
+    run_staged(nchunks, [&](int64_t i, void *buf, cudaEvent_t ev, bool &pending) {
+        const int64_t b = i * kPer, n = std::min(kPer, count - b);
+        if (pending) VK_CUDA(cudaEventSynchronize(ev));
+        int *o = static_cast<int *>(buf);
+        const int64_t *in = src + b;
+        for (int64_t k = 0; k < n; ++k) o[k] = static_cast<int>(in[k]);
+        VK_CUDA(cudaMemcpyAsync(dst + b, buf, n * sizeof(int), cudaMemcpyHostToDevice, s));
+        VK_CUDA(cudaEventRecord(ev, s));
+        pending = true;
+    });
+}
+
+void stage_d2h(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+    if (bytes == 0) return;
+    if (bytes < kStageMin) {
+        VK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+        VK_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    char *h = static_cast<char *>(dst);
+    const char *d = static_cast<const char *>(src);
+    const int64_t nchunks = static_cast<int64_t>((bytes + kStageChunk - 1) / kStageChunk);
+    run_staged(nchunks, [&](int64_t i, void *buf, cudaEvent_t ev, bool &pending) {
+        const size_t off = static_cast<size_t>(i) * kStageChunk;
+        const size_t n = std::min(kStageChunk, bytes - off);
+        VK_CUDA(cudaMemcpyAsync(buf, d + off, n, cudaMemcpyDeviceToHost, s));
+        VK_CUDA(cudaEventRecord(ev, s));
+        pending = true;
+        VK_CUDA(cudaEventSynchronize(ev));
+        pending = false;
+        std::memcpy(h + off, buf, n);
+    });
+}
+
+} // namespace vk
