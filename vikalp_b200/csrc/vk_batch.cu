@@ -14,12 +14,14 @@
 // chunk of check_every iterations is one CUDA graph.
 #include "vk_blockdiag.cuh"
 #include "vk_engine.cuh"
+#include "vk_stage.cuh"
 
 #include <algorithm>
 #include <cmath>
 #include <limits>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <type_traits>
 
 namespace vk {
@@ -485,9 +487,8 @@ public:
         if (m_ > 0) bunscale_kernel<double><<<grid1d(m_), 256, 0, s_>>>(s64_.yhat.get(), rs_.get(), m_, yo.get());
         VK_LAUNCH_CHECK();
         std::vector<double> hx(n_), hy(m_);
-        VK_CUDA(cudaMemcpyAsync(hx.data(), xo.get(), n_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
-        if (m_ > 0) VK_CUDA(cudaMemcpyAsync(hy.data(), yo.get(), m_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
-        VK_CUDA(cudaStreamSynchronize(s_));
+        stage_d2h(hx.data(), xo.get(), n_ * sizeof(double), s_);
+        if (m_ > 0) stage_d2h(hy.data(), yo.get(), m_ * sizeof(double), s_);
         const double secs = seconds_since(started);
         for (int b = 0; b < B_; ++b) {
             vk_result &r = results[b];
@@ -1516,22 +1517,43 @@ public:
         std::vector<int> invalid(B_, 0);
         std::vector<std::string> why(B_);
         std::vector<char> overridden(n, 0);
-        for (int b = 0; b < B_; ++b) {
-            const size_t o = static_cast<size_t>(b) * n;
-            for (int j = 0; j < n && !invalid[b]; ++j) {
-                const double l = lower ? lower[o + j] : model_.var_lower[j];
-                const double u = upper ? upper[o + j] : model_.var_upper[j];
-                if ((lower && std::isnan(lower[o + j])) || (upper && std::isnan(upper[o + j]))) {
-                    invalid[b] = 1;
-                    why[b] = "variable bound overrides must be empty or sized and non-NaN";
-                } else if (std::isnan(l) || std::isnan(u) || l > u) {
-                    invalid[b] = 1;
-                    why[b] = "variable bound overrides contain an invalid interval";
-                } else if (warm && !std::isfinite(warm[o + j])) {
-                    invalid[b] = 1;
-                    why[b] = "warm start must be empty or finite and sized to the model";
+        // instances [b0, b1); `ovr` marks the columns whose bounds differ from the model's
+        auto check = [&](int b0, int b1, std::vector<char> &ovr) {
+            for (int b = b0; b < b1; ++b) {
+                const size_t o = static_cast<size_t>(b) * n;
+                for (int j = 0; j < n && !invalid[b]; ++j) {
+                    const double l = lower ? lower[o + j] : model_.var_lower[j];
+                    const double u = upper ? upper[o + j] : model_.var_upper[j];
+                    if ((lower && std::isnan(lower[o + j])) || (upper && std::isnan(upper[o + j]))) {
+                        invalid[b] = 1;
+                        why[b] = "variable bound overrides must be empty or sized and non-NaN";
+                    } else if (std::isnan(l) || std::isnan(u) || l > u) {
+                        invalid[b] = 1;
+                        why[b] = "variable bound overrides contain an invalid interval";
+                    } else if (warm && !std::isfinite(warm[o + j])) {
+                        invalid[b] = 1;
+                        why[b] = "warm start must be empty or finite and sized to the model";
+                    }
+                    if (l != model_.var_lower[j] || u != model_.var_upper[j]) ovr[j] = 1;
                 }
-                if (l != model_.var_lower[j] || u != model_.var_upper[j]) overridden[j] = 1;
+            }
+        };
+        {
+            // instances split over host threads (each its own column marks)
+            const unsigned hw = std::thread::hardware_concurrency();
+            const int64_t work = static_cast<int64_t>(B_) * n;
+            const int T = work < (int64_t(1) << 20) ? 1 : std::min<int>({B_, 16, static_cast<int>(hw == 0 ? 1 : hw)});
+            std::vector<std::vector<char>> marks(T, std::vector<char>(T > 1 ? n : 0, 0));
+            if (T <= 1) {
+                check(0, B_, overridden);
+            } else {
+                std::vector<std::thread> pool;
+                for (int t = 1; t < T; ++t)
+                    pool.emplace_back([&, t] { check(B_ * t / T, B_ * (t + 1) / T, marks[t]); });
+                check(0, B_ / T, marks[0]);
+                for (std::thread &th : pool) th.join();
+                for (int t = 0; t < T; ++t)
+                    for (int j = 0; j < n; ++j) overridden[j] |= marks[t][j];
             }
         }
         std::vector<int> ov_cols, ov_index(n, -1);
@@ -1552,15 +1574,14 @@ public:
                 const double *model = side == 0 ? model_.var_lower : model_.var_upper;
                 DevBuf<double> &dst = side == 0 ? dlo : dhi;
                 if (src) {
-                    VK_CUDA(cudaMemcpyAsync(dst.get(), src, bn * sizeof(double), cudaMemcpyHostToDevice, s_));
+                    stage_h2d(dst.get(), src, bn * sizeof(double), s_);
                 } else {
                     tmp.resize(bn);
                     for (int b = 0; b < B_; ++b) std::copy(model, model + n, tmp.begin() + static_cast<size_t>(b) * n);
-                    VK_CUDA(cudaMemcpyAsync(dst.get(), tmp.data(), bn * sizeof(double), cudaMemcpyHostToDevice, s_));
-                    VK_CUDA(cudaStreamSynchronize(s_));
+                    stage_h2d(dst.get(), tmp.data(), bn * sizeof(double), s_);
                 }
             }
-            if (warm) VK_CUDA(cudaMemcpyAsync(dwarm.get(), warm, bn * sizeof(double), cudaMemcpyHostToDevice, s_));
+            if (warm) stage_h2d(dwarm.get(), warm, bn * sizeof(double), s_);
         }
         DevBuf<int> dov_index, dov_cols;
         dov_index.reset(n);
@@ -1677,15 +1698,15 @@ public:
         VK_LAUNCH_CHECK();
         std::vector<double> hobj(B_);
         VK_CUDA(cudaMemcpyAsync(hobj.data(), dobj.get(), B_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
+        std::vector<StageCopy> copies;
+        copies.reserve(2 * static_cast<size_t>(B_));
         for (int b = 0; b < B_; ++b) {
             if (invalid[b]) continue;
-            if (results[b].x)
-                VK_CUDA(cudaMemcpyAsync(results[b].x, xo.get() + static_cast<size_t>(b) * n, n * sizeof(double),
-                                        cudaMemcpyDeviceToHost, s_));
+            if (results[b].x) copies.push_back({results[b].x, xo.get() + static_cast<size_t>(b) * n, n * sizeof(double)});
             if (results[b].y && m > 0)
-                VK_CUDA(cudaMemcpyAsync(results[b].y, yo.get() + static_cast<size_t>(b) * m, m * sizeof(double),
-                                        cudaMemcpyDeviceToHost, s_));
+                copies.push_back({results[b].y, yo.get() + static_cast<size_t>(b) * m, m * sizeof(double)});
         }
+        stage_d2h_many(copies.data(), static_cast<int64_t>(copies.size()), s_);
         VK_CUDA(cudaStreamSynchronize(s_));
         lg.mark("results to host");
         const double secs = seconds_since(started);

@@ -1,4 +1,5 @@
 #include "vk_blockdiag.cuh"
+#include "vk_stage.cuh"
 
 #include <algorithm>
 
@@ -97,8 +98,7 @@ void upload_block_diag(const BlockDiag &h, DeviceBlockDiag &d, cudaStream_t s, b
     build_tiles(d.a, s, drb.get());
     d.a_val.reset(padded(h.nnz));
     VK_CUDA(cudaMemsetAsync(d.a_val.get(), 0, padded(h.nnz) * sizeof(double), s));
-    if (h.nnz > 0)
-        VK_CUDA(cudaMemcpyAsync(d.a_val.get(), h.v.data(), h.nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+    stage_h2d(d.a_val.get(), h.v.data(), h.nnz * sizeof(double), s);
     transpose_pattern(d.a, d.at, d.perm, s);
     build_tiles(d.at, s, dcb.get());
     d.at_val.reset(padded(h.nnz));

@@ -145,4 +145,30 @@ void stage_d2h(void *dst, const void *src, size_t bytes, cudaStream_t s) {
     });
 }
 
+void stage_d2h_many(const StageCopy *copies, int64_t count, cudaStream_t s) {
+    size_t total = 0;
+    for (int64_t i = 0; i < count; ++i) total += copies[i].bytes;
+    if (total == 0) return;
+    if (total < kStageMin) {
+        for (int64_t i = 0; i < count; ++i)
+            if (copies[i].bytes > 0)
+                VK_CUDA(cudaMemcpyAsync(copies[i].dst, copies[i].src, copies[i].bytes, cudaMemcpyDeviceToHost, s));
+        VK_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    run_staged(count, [&](int64_t i, void *buf, cudaEvent_t ev, bool &pending) {
+        char *h = static_cast<char *>(copies[i].dst);
+        const char *d = static_cast<const char *>(copies[i].src);
+        for (size_t off = 0; off < copies[i].bytes; off += kStageChunk) {
+            const size_t n = std::min(kStageChunk, copies[i].bytes - off);
+            VK_CUDA(cudaMemcpyAsync(buf, d + off, n, cudaMemcpyDeviceToHost, s));
+            VK_CUDA(cudaEventRecord(ev, s));
+            pending = true;
+            VK_CUDA(cudaEventSynchronize(ev));
+            pending = false;
+            std::memcpy(h + off, buf, n);
+        }
+    });
+}
+
 } // namespace vk

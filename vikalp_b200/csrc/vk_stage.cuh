@@ -29,4 +29,14 @@ void stage_h2d_narrow(int *dst, const int64_t *src, int64_t count, cudaStream_t 
 // complete before the copy starts.
 void stage_d2h(void *dst, const void *src, size_t bytes, cudaStream_t s);
 
+// Many device -> host copies (e.g. one result array per batch instance),
+// spread over the staging threads: copy i goes to thread i % T, in pieces of
+// at most kStageChunk bytes. Staged when the copies add up to kStageMin bytes.
+struct StageCopy {
+    void *dst;
+    const void *src;
+    size_t bytes;
+};
+void stage_d2h_many(const StageCopy *copies, int64_t count, cudaStream_t s);
+
 } // namespace vk
