@@ -216,24 +216,32 @@ def batched_figures(sample_every=64):
                        "(m log-uniform 500..20000, n=2m, 8/col; 19.7M nnz), to 1e-6 relative KKT",
            "mixed": run("mixed"), "fp64_batched": run("fp64")}
     # plain float64, one instance at a time (sample)
+    # each sampled instance is solved twice and keeps the faster time, so a
+    # stall of the host in one of the two runs does not enter the estimate
     node_t, indep_t = [], []
+
+    def best_of_two(run):
+        ts = []
+        for _ in range(2):
+            t = time.perf_counter()
+            r = run()
+            ts.append(time.perf_counter() - t)
+            assert r["status"] == "Optimal", r["status"]
+        return min(ts)
+
     with vk.Pdhg(node_lp, algorithm="halpern", precision="fp64", **tol) as h:
         for b in range(0, 512, sample_every):
-            t = time.perf_counter()
-            r = h.solve(lower=lo[b], upper=hi[b], duals=False)
-            node_t.append(time.perf_counter() - t)
-            assert r["status"] == "Optimal", r["status"]
+            node_t.append(best_of_two(lambda: h.solve(lower=lo[b], upper=hi[b], duals=False)))
     # one untimed create + solve first (an instance outside the sample), so the
     # first sample carries no one-time cost of the path
     vk.solve(indep[1], algorithm="halpern", precision="fp64", **tol)
     for b in range(0, 256, sample_every // 2):
-        t = time.perf_counter()
-        r = vk.solve(indep[b], algorithm="halpern", precision="fp64", **tol)
-        indep_t.append(time.perf_counter() - t)
+        indep_t.append(best_of_two(lambda: vk.solve(indep[b], algorithm="halpern", precision="fp64", **tol)))
     est = 512 * statistics.mean(node_t) + 256 * statistics.mean(indep_t)
     out["plain_fp64_one_by_one"] = {"estimated_s": round(est, 3), "node_sample_s": [round(t, 4) for t in node_t],
                                     "independent_sample_s": [round(t, 4) for t in indep_t],
-                                    "sample": f"{len(node_t)} of 512 nodes, {len(indep_t)} of 256 LPs, mean x count"}
+                                    "sample": f"{len(node_t)} of 512 nodes, {len(indep_t)} of 256 LPs, each the faster of two solves; "
+                                                                          "mean x count"}
     out["speedup_mixed_batched_vs_plain_fp64"] = round(est / out["mixed"]["wall_s"], 2)
     return out
 

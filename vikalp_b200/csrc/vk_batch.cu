@@ -1505,8 +1505,11 @@ public:
         skc_.reset(static_cast<size_t>(B_) * 4);
     }
     ~SharedEngine() {
+        const auto t0 = std::chrono::steady_clock::now();
         if (g64_) cudaGraphExecDestroy(g64_);
         if (g32_) cudaGraphExecDestroy(g32_);
+        if (o_.verbose > 0)
+            std::fprintf(stderr, "[vikalp_b200] shared: graphs destroyed          %8.3f s\n", seconds_since(t0));
     }
 
     void solve(const double *lower, const double *upper, const double *warm, vk_result *results) {
@@ -2052,12 +2055,16 @@ void batch_solve_shared(const vk_problem &p, int count, const double *lower, con
     if ((p.A.cols + 1) * ld >= (int64_t(1) << 40) || count >= (1 << 24))
         throw Unsupported("the batch is too large for one device");
     const auto t0 = std::chrono::steady_clock::now();
+    std::chrono::steady_clock::time_point t1;
     {
         SharedEngine eng(p, count, o);
         eng.solve(lower, upper, warm, results);
+        t1 = std::chrono::steady_clock::now();
     }
-    if (o.verbose > 0)
+    if (o.verbose > 0) {
+        std::fprintf(stderr, "[vikalp_b200] shared: release (graphs, memory)  %8.3f s\n", seconds_since(t1));
         std::fprintf(stderr, "[vikalp_b200] shared: total incl. release      %8.3f s\n", seconds_since(t0));
+    }
 }
 
 } // namespace vk
