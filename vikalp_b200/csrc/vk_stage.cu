@@ -2,6 +2,7 @@
 #include "vk_stage.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <exception>
 #include <mutex>
@@ -36,6 +37,52 @@ void release_pinned(void *p) {
     g_pool.push_back(p);
 }
 
+// 0: pool not started, 1: being allocated, 2: ready, 3: pinned memory unavailable
+std::atomic<int> g_pool_state{0};
+
+// The allocating thread; joined at process exit (function-local static, so
+// destroyed before the CUDA runtime linked into this library shuts down).
+struct PoolWarmup {
+    std::thread t;
+    ~PoolWarmup() {
+        if (t.joinable()) t.join();
+    }
+};
+PoolWarmup &pool_warmup() {
+    static PoolWarmup w;
+    return w;
+}
+
+// True once the pool holds a buffer per staging thread; the first call starts
+// the allocation on a background thread and returns false.
+bool pool_ready() {
+    int st = g_pool_state.load();
+    if (st == 2) return true;
+    if (st == 0 && g_pool_state.compare_exchange_strong(st, 1)) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) {
+            g_pool_state.store(3);
+            return false;
+        }
+        pool_warmup().t = std::thread([dev] {
+            std::vector<void *> bufs;
+            if (cudaSetDevice(dev) == cudaSuccess)
+                for (int i = 0; i < kStageThreads; ++i) {
+                    void *p = nullptr;
+                    if (cudaHostAlloc(&p, kStageChunk, cudaHostAllocPortable) != cudaSuccess) break;
+                    bufs.push_back(p);
+                }
+            const bool ok = static_cast<int>(bufs.size()) == kStageThreads;
+            {
+                std::lock_guard<std::mutex> lk(g_pool_mu);
+                for (void *p : bufs) g_pool.push_back(p);
+            }
+            g_pool_state.store(ok ? 2 : 3);
+        });
+    }
+    return false;
+}
+
 // Runs body(chunk, buffer, event, pending) for chunks 0..nchunks-1, chunk i on
 // thread i % T, each thread with its own pinned buffer and event; `pending`
 // says the buffer's last DMA may still be running. A thread waits for its
@@ -56,8 +103,7 @@ void run_staged(int64_t nchunks, Body body) {
         try {
             VK_CUDA(cudaSetDevice(dev));
             buf = acquire_pinned();
-            // blocking sync: a waiting thread sleeps instead of spinning on a core
-            VK_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming | cudaEventBlockingSync));
+            VK_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
             for (int64_t i = t; i < nchunks; i += T) body(i, buf, ev, pending);
             if (pending) VK_CUDA(cudaEventSynchronize(ev));
             pending = false;
@@ -77,11 +123,17 @@ void run_staged(int64_t nchunks, Body body) {
         if (e) std::rethrow_exception(e);
 }
 
+__global__ void narrow_kernel(const int64_t *__restrict__ src, int *__restrict__ dst, int64_t n) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        dst[i] = static_cast<int>(src[i]);
+}
+
 } // namespace
 
 void stage_h2d(void *dst, const void *src, size_t bytes, cudaStream_t s) {
     if (bytes == 0) return;
-    if (bytes < kStageMin) {
+    if (bytes < kStageMin || !pool_ready()) {
         VK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
         VK_CUDA(cudaStreamSynchronize(s));
         return;
@@ -110,6 +162,16 @@ void stage_h2d_narrow(int *dst, const int64_t *src, int64_t count, cudaStream_t 
         VK_CUDA(cudaStreamSynchronize(s));
         return;
     }
+    if (!pool_ready()) {
+        // plain copy of the int64 values, narrowed on the device
+        DevBuf<int64_t> t(static_cast<size_t>(count));
+        VK_CUDA(cudaMemcpyAsync(t.get(), src, count * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+        const int64_t blocks = std::min<int64_t>((count + 255) / 256, 65535);
+        narrow_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(t.get(), dst, count);
+        VK_LAUNCH_CHECK();
+        VK_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
     const int64_t nchunks = (count + kPer - 1) / kPer;
     run_staged(nchunks, [&](int64_t i, void *buf, cudaEvent_t ev, bool &pending) {
         const int64_t b = i * kPer, n = std::min(kPer, count - b);
@@ -125,7 +187,7 @@ void stage_h2d_narrow(int *dst, const int64_t *src, int64_t count, cudaStream_t 
 
 void stage_d2h(void *dst, const void *src, size_t bytes, cudaStream_t s) {
     if (bytes == 0) return;
-    if (bytes < kStageMin) {
+    if (bytes < kStageMin || !pool_ready()) {
         VK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
         VK_CUDA(cudaStreamSynchronize(s));
         return;
@@ -149,7 +211,7 @@ void stage_d2h_many(const StageCopy *copies, int64_t count, cudaStream_t s) {
     size_t total = 0;
     for (int64_t i = 0; i < count; ++i) total += copies[i].bytes;
     if (total == 0) return;
-    if (total < kStageMin) {
+    if (total < kStageMin || !pool_ready()) {
         for (int64_t i = 0; i < count; ++i)
             if (copies[i].bytes > 0)
                 VK_CUDA(cudaMemcpyAsync(copies[i].dst, copies[i].src, copies[i].bytes, cudaMemcpyDeviceToHost, s));

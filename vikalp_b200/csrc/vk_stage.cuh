@@ -9,14 +9,17 @@
 // DMA before refilling the buffer. The host copies run in parallel and the
 // DMA engine streams at PCIe rate. Every function returns when the transfer
 // has completed (the caller's memory may be reused at once). Copies below
-// kStageMin bytes go straight through cudaMemcpyAsync + a stream wait.
+// kStageMin bytes go straight through cudaMemcpyAsync + a stream wait, and so
+// do all copies until the pinned buffers exist: the first large transfer of
+// the process starts their allocation on a background thread (pinning costs
+// ~0.1 s the first time) and does not wait for it.
 #pragma once
 
 #include "vk_common.cuh"
 
 namespace vk {
 
-constexpr size_t kStageChunk = size_t(8) << 20; // bytes per staged chunk
+constexpr size_t kStageChunk = size_t(4) << 20; // bytes per staged chunk (and per pinned buffer)
 constexpr size_t kStageMin = size_t(16) << 20;  // smaller transfers are not staged
 constexpr int kStageThreads = 4;
 
