@@ -192,6 +192,21 @@ def test_batch_names_the_invalid_member():
     assert msg == "instance 1: variable bounds contains an invalid bound at index 0"
 
 
+def test_batch_first_invalid_member_in_order():
+    # batches of 8 or more members are checked over host threads; the member
+    # reported is still the first invalid one in order
+    bad_bounds = dict(var_lower=np.array([3.0]), var_upper=np.array([2.0]))
+    models = [M() for _ in range(40)]
+    models[29] = M(c=np.array([np.inf]))
+    models[17] = M(**bad_bounds)
+    models[35] = M(**bad_bounds)
+    code, msg = batch_error(models)
+    assert code == vk.VK_ERR_INVALID
+    assert msg == "instance 17: variable bounds contains an invalid bound at index 0"
+    models[4] = M(c=np.array([np.nan]))
+    assert batch_error(models)[1] == "instance 4: objective coefficients must be finite"
+
+
 def test_batch_requires_halpern_and_lp():
     code, _ = batch_error([M()], algorithm="reference")
     assert code == vk.VK_ERR_UNSUPPORTED

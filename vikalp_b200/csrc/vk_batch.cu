@@ -17,6 +17,7 @@
 #include "vk_stage.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <limits>
 #include <numeric>
@@ -2010,13 +2011,31 @@ private:
 void batch_solve(const vk_problem *probs, int count, const vk_options &o, vk_result *results) {
     if (count <= 0) throw InvalidInput("count must be positive");
     if (o.algorithm != VK_ALGO_HALPERN) throw Unsupported("batched solves use VK_ALGO_HALPERN");
+    // every instance checked (over host threads for large batches); the
+    // first failing instance in order is reported, as a sequential scan would
+    std::vector<std::string> msgs(count);
+    std::vector<char> unsup(count, 0);
+    {
+        std::atomic<int> next{0};
+        auto work = [&] {
+            for (int b = next++; b < count; b = next++) {
+                bool unsupported = false;
+                msgs[b] = validate_problem(probs[b], o, unsupported);
+                unsup[b] = unsupported ? 1 : 0;
+            }
+        };
+        const unsigned hw = std::thread::hardware_concurrency();
+        const int T = count < 8 ? 1 : std::min<int>({count, 16, static_cast<int>(hw == 0 ? 1 : hw)});
+        std::vector<std::thread> pool;
+        for (int t = 1; t < T; ++t) pool.emplace_back(work);
+        work();
+        for (std::thread &th : pool) th.join();
+    }
     int64_t m = 0, n = 0, nnz = 0;
     for (int b = 0; b < count; ++b) {
-        bool unsupported = false;
-        const std::string msg = validate_problem(probs[b], o, unsupported);
-        if (!msg.empty()) {
-            const std::string full = "instance " + std::to_string(b) + ": " + msg;
-            if (unsupported) throw Unsupported(full);
+        if (!msgs[b].empty()) {
+            const std::string full = "instance " + std::to_string(b) + ": " + msgs[b];
+            if (unsup[b]) throw Unsupported(full);
             throw InvalidInput(full);
         }
         if (probs[b].Q.rows > 0 && probs[b].Q.row_offsets && probs[b].Q.row_offsets[probs[b].Q.rows] > 0)

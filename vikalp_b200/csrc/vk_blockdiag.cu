@@ -2,8 +2,39 @@
 #include "vk_stage.cuh"
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
+#include <vector>
 
 namespace vk {
+
+namespace {
+
+// Instance b's rows, columns and nonzeros at its offsets in the concatenation.
+void fill_instance(const vk_problem &p, int b, BlockDiag &out) {
+    const int r0 = out.row_off[b], c0 = out.col_off[b];
+    const int64_t k0 = out.nnz_off[b];
+    for (int64_t i = 0; i < p.A.rows; ++i) {
+        out.ro[r0 + i + 1] = k0 + p.A.row_offsets[i + 1];
+        out.rinst[r0 + i] = b;
+        out.rl[r0 + i] = p.row_lower[i];
+        out.ru[r0 + i] = p.row_upper[i];
+    }
+    const int64_t nz = out.nnz_off[b + 1] - k0;
+    for (int64_t k = 0; k < nz; ++k) {
+        out.ci[k0 + k] = c0 + p.A.col_indices[k];
+        out.v[k0 + k] = p.A.values[k];
+    }
+    for (int64_t j = 0; j < p.A.cols; ++j) {
+        out.c[c0 + j] = p.c[j];
+        out.vl[c0 + j] = p.var_lower[j];
+        out.vu[c0 + j] = p.var_upper[j];
+        out.cinst[c0 + j] = b;
+    }
+    out.offset[b] = p.objective_offset;
+}
+
+} // namespace
 
 void concat_instances(const vk_problem *probs, int count, BlockDiag &out) {
     out.count = count;
@@ -32,29 +63,17 @@ void concat_instances(const vk_problem *probs, int count, BlockDiag &out) {
     out.offset.resize(count);
     out.rinst.resize(m);
     out.cinst.resize(n);
-    for (int b = 0; b < count; ++b) {
-        const vk_problem &p = probs[b];
-        const int r0 = out.row_off[b], c0 = out.col_off[b];
-        const int64_t k0 = out.nnz_off[b];
-        for (int64_t i = 0; i < p.A.rows; ++i) {
-            out.ro[r0 + i + 1] = k0 + p.A.row_offsets[i + 1];
-            out.rinst[r0 + i] = b;
-            out.rl[r0 + i] = p.row_lower[i];
-            out.ru[r0 + i] = p.row_upper[i];
-        }
-        const int64_t nz = out.nnz_off[b + 1] - k0;
-        for (int64_t k = 0; k < nz; ++k) {
-            out.ci[k0 + k] = c0 + p.A.col_indices[k];
-            out.v[k0 + k] = p.A.values[k];
-        }
-        for (int64_t j = 0; j < p.A.cols; ++j) {
-            out.c[c0 + j] = p.c[j];
-            out.vl[c0 + j] = p.var_lower[j];
-            out.vu[c0 + j] = p.var_upper[j];
-            out.cinst[c0 + j] = b;
-        }
-        out.offset[b] = p.objective_offset;
-    }
+    // instances write disjoint ranges: large batches fill them over host threads
+    std::atomic<int> next{0};
+    auto fill = [&] {
+        for (int b = next++; b < count; b = next++) fill_instance(probs[b], b, out);
+    };
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int T = nnz < (int64_t(1) << 20) || count < 2 ? 1 : std::min<int>({count, 16, static_cast<int>(hw == 0 ? 1 : hw)});
+    std::vector<std::thread> pool;
+    for (int t = 1; t < T; ++t) pool.emplace_back(fill);
+    fill();
+    for (std::thread &th : pool) th.join();
 }
 
 namespace {

@@ -85,11 +85,12 @@ bool pool_ready() {
 
 // Runs body(chunk, buffer, event, pending) for chunks 0..nchunks-1, chunk i on
 // thread i % T, each thread with its own pinned buffer and event; `pending`
-// says the buffer's last DMA may still be running. A thread waits for its
-// last DMA before its buffer goes back to the pool, also after an error; the
-// first error is rethrown on the calling thread.
+// says a DMA touching the buffer may still be running (set before its event
+// is recorded). A thread waits for its last DMA before its buffer goes back to
+// the pool; after an error it waits for the whole stream s. The first error is
+// rethrown on the calling thread.
 template <class Body>
-void run_staged(int64_t nchunks, Body body) {
+void run_staged(int64_t nchunks, cudaStream_t s, Body body) {
     int dev = 0;
     VK_CUDA(cudaGetDevice(&dev));
     const unsigned hw = std::thread::hardware_concurrency();
@@ -109,8 +110,9 @@ void run_staged(int64_t nchunks, Body body) {
             pending = false;
         } catch (...) {
             errs[t] = std::current_exception();
+            if (pending) cudaStreamSynchronize(s);
+            pending = false;
         }
-        if (pending) cudaEventSynchronize(ev);
         if (ev) cudaEventDestroy(ev);
         if (buf) release_pinned(buf);
     };
@@ -141,14 +143,14 @@ void stage_h2d(void *dst, const void *src, size_t bytes, cudaStream_t s) {
     char *d = static_cast<char *>(dst);
     const char *h = static_cast<const char *>(src);
     const int64_t nchunks = static_cast<int64_t>((bytes + kStageChunk - 1) / kStageChunk);
-    run_staged(nchunks, [&](int64_t i, void *buf, cudaEvent_t ev, bool &pending) {
+    run_staged(nchunks, s, [&](int64_t i, void *buf, cudaEvent_t ev, bool &pending) {
         const size_t off = static_cast<size_t>(i) * kStageChunk;
         const size_t n = std::min(kStageChunk, bytes - off);
         if (pending) VK_CUDA(cudaEventSynchronize(ev));
         std::memcpy(buf, h + off, n);
+        pending = true;
         VK_CUDA(cudaMemcpyAsync(d + off, buf, n, cudaMemcpyHostToDevice, s));
         VK_CUDA(cudaEventRecord(ev, s));
-        pending = true;
     });
 }
 
@@ -173,15 +175,15 @@ void stage_h2d_narrow(int *dst, const int64_t *src, int64_t count, cudaStream_t 
         return;
     }
     const int64_t nchunks = (count + kPer - 1) / kPer;
-    run_staged(nchunks, [&](int64_t i, void *buf, cudaEvent_t ev, bool &pending) {
+    run_staged(nchunks, s, [&](int64_t i, void *buf, cudaEvent_t ev, bool &pending) {
         const int64_t b = i * kPer, n = std::min(kPer, count - b);
         if (pending) VK_CUDA(cudaEventSynchronize(ev));
         int *o = static_cast<int *>(buf);
         const int64_t *in = src + b;
         for (int64_t k = 0; k < n; ++k) o[k] = static_cast<int>(in[k]);
+        pending = true;
         VK_CUDA(cudaMemcpyAsync(dst + b, buf, n * sizeof(int), cudaMemcpyHostToDevice, s));
         VK_CUDA(cudaEventRecord(ev, s));
-        pending = true;
     });
 }
 
@@ -195,12 +197,12 @@ void stage_d2h(void *dst, const void *src, size_t bytes, cudaStream_t s) {
     char *h = static_cast<char *>(dst);
     const char *d = static_cast<const char *>(src);
     const int64_t nchunks = static_cast<int64_t>((bytes + kStageChunk - 1) / kStageChunk);
-    run_staged(nchunks, [&](int64_t i, void *buf, cudaEvent_t ev, bool &pending) {
+    run_staged(nchunks, s, [&](int64_t i, void *buf, cudaEvent_t ev, bool &pending) {
         const size_t off = static_cast<size_t>(i) * kStageChunk;
         const size_t n = std::min(kStageChunk, bytes - off);
+        pending = true;
         VK_CUDA(cudaMemcpyAsync(buf, d + off, n, cudaMemcpyDeviceToHost, s));
         VK_CUDA(cudaEventRecord(ev, s));
-        pending = true;
         VK_CUDA(cudaEventSynchronize(ev));
         pending = false;
         std::memcpy(h + off, buf, n);
@@ -218,14 +220,14 @@ void stage_d2h_many(const StageCopy *copies, int64_t count, cudaStream_t s) {
         VK_CUDA(cudaStreamSynchronize(s));
         return;
     }
-    run_staged(count, [&](int64_t i, void *buf, cudaEvent_t ev, bool &pending) {
+    run_staged(count, s, [&](int64_t i, void *buf, cudaEvent_t ev, bool &pending) {
         char *h = static_cast<char *>(copies[i].dst);
         const char *d = static_cast<const char *>(copies[i].src);
         for (size_t off = 0; off < copies[i].bytes; off += kStageChunk) {
             const size_t n = std::min(kStageChunk, copies[i].bytes - off);
+            pending = true;
             VK_CUDA(cudaMemcpyAsync(buf, d + off, n, cudaMemcpyDeviceToHost, s));
             VK_CUDA(cudaEventRecord(ev, s));
-            pending = true;
             VK_CUDA(cudaEventSynchronize(ev));
             pending = false;
             std::memcpy(h + off, buf, n);
