@@ -207,7 +207,7 @@ int vk_spmat_apply_device(vk_spmat *m, const void *x_device, void *y_device, int
 int64_t vk_spmat_bytes(const vk_spmat *m, int transpose);
 /* Kernel variant the setup autotuner picked for A (transpose == 0) or A'
  * (timing each candidate on this matrix), and a way to pin one
- * (0 <= variant < 17). Results agree to rounding across variants. */
+ * (0 <= variant < 18). Results agree to rounding across variants. */
 int vk_spmat_variant(const vk_spmat *m, int transpose);
 int vk_spmat_set_variant(vk_spmat *m, int transpose, int variant);
 void vk_spmat_destroy(vk_spmat *m);

@@ -37,7 +37,7 @@ _i64p = C.POINTER(C.c_int64)
 _f64p = C.POINTER(C.c_double)
 
 
-FAST_VARIANTS = 17  # kernel variants of the sparse pass (vk_spmat_set_variant)
+FAST_VARIANTS = 18  # kernel variants of the sparse pass (vk_spmat_set_variant)
 
 
 class VkError(RuntimeError):

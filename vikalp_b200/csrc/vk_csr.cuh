@@ -159,7 +159,7 @@ struct Gathers {
 struct FastVariant {
     int u, pipe, minb, sub, hyb, stage = 0, late = 0;
 };
-constexpr int kFastVariants = 17;
+constexpr int kFastVariants = 18;
 constexpr int kTuneRounds = 4;    // timed rounds per variant in the autotuners
 constexpr float kTuneKeep = 1.25f; // variants slower than this x the best leave after the first timed round
 __host__ __device__ constexpr FastVariant fast_variant(int v) {
@@ -179,7 +179,8 @@ __host__ __device__ constexpr FastVariant fast_variant(int v) {
            : v == 13 ? FastVariant{2, 0, 16, 8, 2}
            : v == 14 ? FastVariant{4, 0, 16, 4, 1}
            : v == 15 ? FastVariant{2, 0, 16, 8, 2, 0, 1}
-                     : FastVariant{2, 0, 16, 4, 1, 0, 1};
+           : v == 16 ? FastVariant{2, 0, 16, 4, 1, 0, 1}
+                     : FastVariant{2, 0, 16, 16, 2, 0, 1};
 }
 
 template <class T, class A, int NV, class Epi, int U, bool PIPE, int MINB>
@@ -1047,6 +1048,7 @@ inline int launch_tiles(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi 
     case 14: return launch_fast<T, A, NV, Epi, 14>(M, g, epi, s);
     case 15: return launch_fast<T, A, NV, Epi, 15>(M, g, epi, s);
     case 16: return launch_fast<T, A, NV, Epi, 16>(M, g, epi, s);
+    case 17: return launch_fast<T, A, NV, Epi, 17>(M, g, epi, s);
 
     default: return launch_fast<T, A, NV, Epi, 0>(M, g, epi, s);
     }

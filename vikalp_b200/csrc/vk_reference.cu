@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <limits>
 #include <vector>
 
@@ -651,6 +652,16 @@ private:
         if (const int f = forced_variant(); f >= 0) {
             col_variant_ = row_variant_ = f;
             return;
+        }
+        // VIKALP_B200_PASS_VARIANTS=<column>,<row> pins the two fused passes
+        // alone (profiling runs that must launch what a tuned run launches)
+        if (const char *e = std::getenv("VIKALP_B200_PASS_VARIANTS"); e && *e) {
+            int c = -1, r = -1;
+            if (std::sscanf(e, "%d,%d", &c, &r) == 2 && c >= 0 && c < kFastVariants && r >= 0 && r < kFastVariants) {
+                col_variant_ = c;
+                row_variant_ = r;
+                return;
+            }
         }
         if (exact_ || dm_.nnz < 200000 || dm_.m == 0) return;
         prepare(nullptr, dm_.vl.get(), dm_.vu.get(), std::numeric_limits<long long>::max() / 4, 0.0);
