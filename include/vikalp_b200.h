@@ -276,6 +276,20 @@ int vk_vec_norm_inf_device(const double *x_device, int64_t n, double *result_dev
 int vk_vec_dot_device_noalloc(const double *x_device, const double *y_device, int64_t n, double *result_device,
                               void *stream);
 
+/* ---- diagnostics ------------------------------------------------------------ */
+
+/* Runs the library's failure path for a device wait that never completes,
+ * without a fault: one kernel polls an mbarrier that nothing arrives on,
+ * `polls` times at most (1..1048576; each poll may suspend the thread
+ * briefly), the way the pipelined sparse passes wait for their staged copies.
+ * When the limit runs out the kernel records the barrier-timeout code in the
+ * per-device error flag and returns; the host reads and clears the flag as
+ * after every solve chunk. Expected result: VK_ERR_CUDA with the timeout
+ * message (vk_last_error), and the device stays usable for the next call.
+ * No counterpart in the reference (its CUDA backend has no device-side waits;
+ * failures there are exceptions, cuda_ops.cu:35-46). */
+int vk_diag_bounded_wait(int32_t polls);
+
 /* ---- batches ---------------------------------------------------------------- */
 
 /* Solves `count` independent LPs (any sizes) together with VK_ALGO_HALPERN

@@ -205,7 +205,7 @@ class Reference:
 
     def __init__(self, path: str = REF_SO):
         if not os.path.exists(path):
-            raise FileNotFoundError(f"{path} missing: build it with `make -C oracle ref` where the reference tree exists")
+            raise FileNotFoundError(f"{path} missing: build it with `make -C oracle ref REF=<reference tree>`")
         lib = C.CDLL(path)
         lib.vkref_solve_continuous.restype = C.c_int
         lib.vkref_solve_continuous.argtypes = [C.POINTER(_RefProblem), C.POINTER(_RefOptions), _f64p,

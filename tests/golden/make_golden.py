@@ -2,7 +2,7 @@
 
 Run from the repository root where the reference tree is present:
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REF=<reference tree> && python tests/golden/make_golden.py
 
 It drives the reference's own CPU code (oracle/_ref/libvkref.so, compiled by
 oracle/Makefile from the reference sources) on

@@ -1,0 +1,71 @@
+"""Same input, same bits: the FAST product order sums in the order of the
+kernel variant the autotuner picked, so two solves of one LP must run the same
+variants. Branch-and-bound callers rely on that (the reference's
+deterministic node-order test, tests/solver/integer/test_mip.cpp:534, assumes
+a relaxation returns the same answer every time it is asked).
+
+The tuner's picks are cached per matrix for the process; these tests create
+separate handles on one LP (each handle tunes on first need, or reuses the
+cached pick) and compare every returned array under ==."""
+
+import time
+
+import numpy as np
+import pytest
+
+import vikalp_b200 as vk
+from conftest import same_bits
+from vikalp_b200 import synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def tuned_lp():
+    # above both tuning thresholds (200k nonzeros for the patterns and the
+    # reference scheme's passes, 2M for the Halpern passes); power-law columns
+    # make the variants' timings differ
+    return synthetic.lp_powerlaw(150_000, 300_000, 2_400_000, seed=77)
+
+
+def _arrays(r):
+    return {k: r[k] for k in ("x", "y", "row_lower_dual", "row_upper_dual", "var_lower_dual", "var_upper_dual")
+            if k in r and r[k] is not None}
+
+
+def test_reference_fast_order_two_handles_same_bits(tuned_lp):
+    runs = []
+    for _ in range(3):
+        with vk.Pdhg(tuned_lp, algorithm="reference", spmv_order="fast") as h:
+            runs.append(h.solve(iteration_limit=300, primal_tolerance=0.0, dual_tolerance=0.0))
+    for r in runs[1:]:
+        assert r["iterations"] == runs[0]["iterations"] == 300
+        for k, v in _arrays(runs[0]).items():
+            assert same_bits(r[k], v), k
+        assert same_bits(r["objective"], runs[0]["objective"])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_halpern_two_handles_same_bits(tuned_lp, precision):
+    runs = []
+    for _ in range(2):
+        with vk.Pdhg(tuned_lp, algorithm="halpern", precision=precision) as h:
+            runs.append(h.solve(iteration_limit=640, relative_tolerance=0.0, duals=False))
+    assert runs[0]["iterations"] == runs[1]["iterations"] == 640
+    for k in ("x", "y"):
+        assert same_bits(runs[1][k], runs[0][k]), k
+
+
+def test_second_handle_skips_the_tuning(tuned_lp):
+    # the first handle on a new matrix times the variants; a second handle on
+    # the same matrix takes the cached picks, so its create + first solve is
+    # not slower than the first one's (the timing is loose: the point is that
+    # no second round of ~150 timed launches runs)
+    lp = synthetic.lp_powerlaw(150_000, 300_000, 2_400_000, seed=78)
+    ts = []
+    for _ in range(2):
+        t = time.perf_counter()
+        with vk.Pdhg(lp, algorithm="reference", spmv_order="fast") as h:
+            h.solve(iteration_limit=64, primal_tolerance=0.0, dual_tolerance=0.0, duals=False)
+        ts.append(time.perf_counter() - t)
+    assert ts[1] <= ts[0] * 1.5 + 0.05, ts

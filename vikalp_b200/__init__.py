@@ -133,6 +133,7 @@ _SIGNATURES = {
     "vk_default_adjoint_options": (None, [C.POINTER(AdjointOptions)]),
     "vk_lp_adjoint": (C.c_int, [C.POINTER(Problem), C.c_int32, _f64p, _f64p, _f64p, C.c_double,
                                 C.POINTER(AdjointOptions), _f64p, _f64p, _f64p, C.POINTER(AdjointInfo)]),
+    "vk_diag_bounded_wait": (C.c_int, [C.c_int32]),
 }
 
 # include/vikalp_mps.h: the MPS ingest path, exported by the C++ host layer (libvikalp.so).

@@ -424,6 +424,43 @@ int vk_vec_norm_inf_device(const double *x, int64_t n, double *result, void *str
     });
 }
 
+namespace {
+// One CTA; thread 0 waits on an mbarrier that expects one arrival nobody makes,
+// with the same bounded poll the pipelined sparse passes use for their staged
+// copies; on timeout it records the code those passes record and returns.
+__global__ void bounded_wait_probe_kernel(int *err, uint32_t polls, int *gave_up) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        vk::mbar_init(&bar, 1);
+        vk::fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const bool done = vk::mbar_wait_bounded(&bar, 0, polls);
+        if (!done) atomicCAS(err, 0, static_cast<int>(vk::kDevErrBarrierTimeout));
+        *gave_up = done ? 0 : 1;
+        asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(vk::smem_u32(&bar)) : "memory");
+    }
+}
+} // namespace
+
+int vk_diag_bounded_wait(int32_t polls) {
+    return guarded([&] {
+        if (polls < 1 || polls > (1 << 20)) return set_error(VK_ERR_INVALID, "polls must be in [1, 1048576]");
+        Stream st;
+        int *err = vk::device_error_flag();
+        vk::DevBuf<int> gave_up(1);
+        bounded_wait_probe_kernel<<<1, 32, 0, st.s>>>(err, static_cast<uint32_t>(polls), gave_up.get());
+        VK_LAUNCH_CHECK();
+        int h = 0;
+        VK_CUDA(cudaMemcpyAsync(&h, gave_up.get(), sizeof(int), cudaMemcpyDeviceToHost, st.s));
+        // reads and clears the device error flag; throws (-> VK_ERR_CUDA) when set
+        vk::check_device_error(st.s);
+        return h ? set_error(VK_ERR_INTERNAL, "the probe's wait gave up but no device error was recorded")
+                 : set_error(VK_ERR_INTERNAL, "the probe's barrier completed although nothing arrived");
+    });
+}
+
 void vk_spmat_destroy(vk_spmat *m) {
     try {
         delete m;

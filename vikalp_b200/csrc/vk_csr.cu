@@ -5,6 +5,8 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <mutex>
+#include <unordered_map>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -168,6 +170,16 @@ int schedule(const CsrPattern32 &p, cudaStream_t s, const unsigned char *breaks,
 
 void build_tiles(CsrPattern32 &p, cudaStream_t s, const unsigned char *breaks) {
     const int rows = p.rows;
+    if (breaks) {
+        // forced tile starts change the schedule: fold them into the identity
+        std::vector<unsigned char> h(static_cast<size_t>(rows) + 1);
+        VK_CUDA(cudaMemcpyAsync(h.data(), breaks, h.size(), cudaMemcpyDeviceToHost, s));
+        VK_CUDA(cudaStreamSynchronize(s));
+        uint64_t f = 0x62726561u; // "brea"
+        for (size_t r = 0; r < h.size(); ++r)
+            if (h[r]) f = mix_fingerprint(f, r);
+        p.fp = mix_fingerprint(p.fp, f);
+    }
     p.ntiles = schedule(p, s, breaks, kChunk, kShortMax, kTileRows, p.tiles, p.tile_k);
     p.nstiles = schedule(p, s, nullptr, kStageWindow, kStageShort, kStageRows, p.stiles, p.stile_k);
     // cost-balanced row ranges for the hybrid kernel
@@ -198,6 +210,7 @@ void upload_pattern(int64_t rows, int64_t cols, const int64_t *h_ro, const int64
     int mr = 0;
     for (int64_t r = 0; r < rows; ++r) mr = std::max<int>(mr, static_cast<int>(h_ro[r + 1] - h_ro[r]));
     out.max_row = mr;
+    out.fp = pattern_fingerprint(rows, cols, h_ro, h_ci);
     build_tiles(out, s);
 }
 
@@ -212,6 +225,7 @@ void transpose_pattern(const CsrPattern32 &a, CsrPattern32 &at, DevBuf<int> &per
     at.rows = a.cols;
     at.cols = a.rows;
     at.nnz = nnz;
+    at.fp = mix_fingerprint(a.fp, 0x7472616e73706f73ull); // "transpos"
     at.ro.reset(a.cols + 1);
     at.ci.reset(padded(nnz));
     VK_CUDA(cudaMemsetAsync(at.ci.get(), 0, padded(nnz) * sizeof(int), s));
@@ -308,6 +322,60 @@ int forced_variant() {
     return v >= 0 && v < kFastVariants ? v : -1;
 }
 
+uint64_t mix_fingerprint(uint64_t a, uint64_t b) {
+    uint64_t h = a ^ 0x9e3779b97f4a7c15ull;
+    for (int k = 0; k < 8; ++k) {
+        h ^= (b >> (8 * k)) & 0xffu;
+        h *= 0x100000001b3ull;
+    }
+    return h;
+}
+
+uint64_t pattern_fingerprint(int64_t rows, int64_t cols, const int64_t *ro, const int64_t *ci) {
+    uint64_t h = 0xcbf29ce484222325ull;
+    h = mix_fingerprint(h, static_cast<uint64_t>(rows));
+    h = mix_fingerprint(h, static_cast<uint64_t>(cols));
+    for (int64_t r = 0; r <= rows; ++r) h = mix_fingerprint(h, static_cast<uint64_t>(ro[r]));
+    const int64_t nnz = ro[rows];
+    for (int64_t k = 0; k < nnz; k += 61) h = mix_fingerprint(h, static_cast<uint64_t>(ci[k]));
+    if (nnz > 0) h = mix_fingerprint(h, static_cast<uint64_t>(ci[nnz - 1]));
+    return h;
+}
+
+namespace {
+std::mutex g_tune_mu;
+std::unordered_map<uint64_t, int> &tune_cache() {
+    static auto *m = new std::unordered_map<uint64_t, int>(); // lives until exit
+    return *m;
+}
+// the current device and its SM count: picks are per GPU model and device
+uint64_t device_key() {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 0;
+    return (static_cast<uint64_t>(static_cast<uint32_t>(dev)) << 32) | static_cast<uint32_t>(sms);
+}
+} // namespace
+
+uint64_t tune_key(uint64_t fingerprint, const char *tag, int value_bytes) {
+    uint64_t h = mix_fingerprint(fingerprint, device_key());
+    for (const char *c = tag; *c; ++c) h = mix_fingerprint(h, static_cast<unsigned char>(*c));
+    return mix_fingerprint(h, static_cast<uint64_t>(value_bytes));
+}
+
+bool cached_pick(uint64_t key, int &variant) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = tune_cache().find(key);
+    if (it == tune_cache().end()) return false;
+    variant = it->second;
+    return true;
+}
+
+int store_pick(uint64_t key, int variant) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    return tune_cache().emplace(key, variant).first->second;
+}
+
 template <class T>
 void autotune_pattern(CsrPattern32 &p, const T *val, cudaStream_t s, int64_t min_nnz) {
     p.variant = 0;
@@ -316,6 +384,8 @@ void autotune_pattern(CsrPattern32 &p, const T *val, cudaStream_t s, int64_t min
         return;
     }
     if (p.nnz < min_nnz || p.rows == 0 || p.cols == 0) return;
+    const uint64_t key = tune_key(p.fp, "pattern", sizeof(T));
+    if (cached_pick(key, p.variant)) return;
     DevBuf<T> x(p.cols), y(p.rows), pre(static_cast<size_t>(p.rows) * 4);
     fill_kernel<T><<<grid_for(p.cols), 256, 0, s>>>(x.get(), p.cols, T(1));
     fill_kernel<T><<<grid_for(int64_t(p.rows) * 4), 256, 0, s>>>(pre.get(), int64_t(p.rows) * 4, T(1));
@@ -333,7 +403,7 @@ void autotune_pattern(CsrPattern32 &p, const T *val, cudaStream_t s, int64_t min
             launch_tiles<T, T, 1, false>(view(p, val), Gathers<T, 1>{{x.get()}}, e, s);
         },
         s, best);
-    p.variant = best_v;
+    p.variant = store_pick(key, best_v);
 }
 
 template void autotune_pattern<double>(CsrPattern32 &, const double *, cudaStream_t, int64_t);

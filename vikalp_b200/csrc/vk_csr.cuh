@@ -84,6 +84,10 @@ struct CsrPattern32 {
     int ntiles = 0, nchunks = 0, nstiles = 0;
     int max_row = 0;
     int variant = 0; // FAST kernel variant picked by autotune_pattern
+    // Identity of the pattern for the tuning cache (tuned_pick): a hash of
+    // its dimensions, row offsets, a sample of its column indices and its
+    // tile breaks; the transpose derives its own from the source's.
+    uint64_t fp = 0;
 };
 
 // Per-device error flag the kernels write (first error wins).
@@ -162,6 +166,7 @@ struct FastVariant {
 constexpr int kFastVariants = 18;
 constexpr int kTuneRounds = 4;    // timed rounds per variant in the autotuners
 constexpr float kTuneKeep = 1.25f; // variants slower than this x the best leave after the first timed round
+constexpr float kTuneTie = 1.02f;  // variants within this x the fastest count as tied: the lowest index wins
 __host__ __device__ constexpr FastVariant fast_variant(int v) {
     return v == 0   ? FastVariant{4, 1, 12, 0, 0}
            : v == 1 ? FastVariant{8, 1, 8, 0, 0}
@@ -977,12 +982,14 @@ inline int launch_fast(const CsrView<T> &M, const Gathers<T, NV> &g, const Epi &
 }
 
 // Times launch(v) -- one launch of a pass with FAST variant v on stream s --
-// for every variant and returns the fastest: one untimed round, one timed
+// for every variant and returns the pick: one untimed round, one timed
 // round over all variants, then kTuneRounds - 1 rounds over those within
 // kTuneKeep of the best. Rounds interleave the variants (clock drift hits
 // them alike) and each variant keeps its best round in best[v] (a dropped
 // variant: its first timed round). A round's launches queue back to back,
-// one event pair each, and the host waits once per round.
+// one event pair each, and the host waits once per round. The pick is the
+// lowest-numbered variant within kTuneTie of the fastest, so near-ties (which
+// timing noise could order either way) resolve the same way every time.
 template <class L>
 int tune_variants(L &&launch, cudaStream_t s, float (&best)[kFastVariants]) {
     cudaEvent_t ev[2 * kFastVariants];
@@ -1013,6 +1020,9 @@ int tune_variants(L &&launch, cudaStream_t s, float (&best)[kFastVariants]) {
             for (int v = 0; v < kFastVariants; ++v) keep[v] = best[v] <= kTuneKeep * lo;
     }
     for (cudaEvent_t &e : ev) cudaEventDestroy(e);
+    const float lo = *std::min_element(best, best + kFastVariants);
+    for (int v = 0; v < kFastVariants; ++v)
+        if (best[v] <= kTuneTie * lo) return v;
     return static_cast<int>(std::min_element(best, best + kFastVariants) - best);
 }
 
@@ -1116,5 +1126,33 @@ template <class T>
 void autotune_pattern(CsrPattern32 &p, const T *val, cudaStream_t s, int64_t min_nnz = 200000);
 // The pinned variant, or -1.
 int forced_variant();
+
+// Process-wide cache of tuning results. `key` identifies what was tuned: a
+// pattern fingerprint (CsrPattern32::fp) mixed with a tag naming the pass and
+// precision (tune_key). The first call for a key on a device runs tune() and
+// stores its pick; later calls -- another handle on the same matrix, another
+// solve -- return the stored pick without timing anything, so the same input
+// runs the same kernel variant (and gives the same bits) for the life of the
+// process. Thread-safe; if two threads tune one key at once, the first stored
+// pick is the one both return.
+template <class F>
+int tuned_pick(uint64_t key, F &&tune);
+uint64_t tune_key(uint64_t fingerprint, const char *tag, int value_bytes);
+// Looks up a stored pick; false when the key has none yet.
+bool cached_pick(uint64_t key, int &variant);
+// Stores a pick (unless one is stored already) and returns the stored one.
+int store_pick(uint64_t key, int variant);
+
+template <class F>
+int tuned_pick(uint64_t key, F &&tune) {
+    int v = 0;
+    if (cached_pick(key, v)) return v;
+    return store_pick(key, tune());
+}
+
+// Fingerprint of a host CSR pattern (rows, cols, every row offset, every
+// 61st column index and the last one), FNV-1a over 64-bit words.
+uint64_t pattern_fingerprint(int64_t rows, int64_t cols, const int64_t *ro, const int64_t *ci);
+uint64_t mix_fingerprint(uint64_t a, uint64_t b);
 
 } // namespace vk

@@ -557,6 +557,13 @@ public:
         if (forced_variant() >= 0 || dm_.nnz < kTunePassesMinNnz) return;
         for (int pass = 0; pass < (st.m > 0 ? 2 : 1); ++pass) {
             int &var = pass == 0 ? col_var_[q] : row_var_[q];
+            // cached per matrix and precision for the process (tuned_pick)
+            const uint64_t key = tune_key(dm_.a.fp,
+                                          pass == 1 ? "halpern row pass"
+                                          : dm_.qp  ? "halpern column pass, qp"
+                                                    : "halpern column pass",
+                                          sizeof(T));
+            if (cached_pick(key, var)) continue;
             auto launch = [&](int v) {
                 var = v;
                 if (pass == 0)
@@ -565,7 +572,7 @@ public:
                     row_pass<T, false>(st, 0);
             };
             float best[kFastVariants];
-            const int pick = tune_variants(launch, s_, best);
+            const int pick = store_pick(key, tune_variants(launch, s_, best));
             var = pick;
             if (o_.verbose > 0) {
                 std::fprintf(stderr, "[vikalp_b200] halpern %s %s pass variants (ms, best timed round):",

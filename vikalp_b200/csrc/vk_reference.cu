@@ -664,6 +664,15 @@ private:
             }
         }
         if (exact_ || dm_.nnz < 200000 || dm_.m == 0) return;
+        // picks are cached per matrix for the process (tuned_pick): another
+        // handle on the same model runs the same variants, no timing
+        const uint64_t keys[2] = {tune_key(dm_.a.fp, dm_.qp ? "reference column pass, qp" : "reference column pass", 8),
+                                  tune_key(dm_.a.fp, "reference row pass", 8)};
+        if (int c = 0, r = 0; cached_pick(keys[0], c) && cached_pick(keys[1], r)) {
+            col_variant_ = c;
+            row_variant_ = r;
+            return;
+        }
         prepare(nullptr, dm_.vl.get(), dm_.vu.get(), std::numeric_limits<long long>::max() / 4, 0.0);
         for (int pass = 0; pass < 2; ++pass) {
             auto launch = [&](int v) {
@@ -692,7 +701,7 @@ private:
                 }
             };
             float best[kFastVariants];
-            const int pick = tune_variants(launch, s_, best);
+            const int pick = store_pick(keys[pass], tune_variants(launch, s_, best));
             (pass == 0 ? col_variant_ : row_variant_) = pick;
             if (o_.verbose > 0) {
                 std::fprintf(stderr, "[vikalp_b200] %s pass variants (ms, best timed round):",
