@@ -302,9 +302,11 @@ int vk_diag_bounded_wait(int32_t polls);
  * keep their own step sizes, primal weights, restarts and stopping, so each
  * result[b] equals, up to rounding, what one VK_ALGO_HALPERN solve of
  * problem b returns. results[b] receives x, y, status, iterations, restarts,
- * objective and the relative KKT figures; the duals split and the absolute
- * residuals are not computed (NaN). iterate_seconds and kernel_launches cover
- * the whole batch. */
+ * objective and the relative KKT figures. When results[b] also carries any of
+ * the four dual arrays (and x, y), those arrays and the reference's three
+ * absolute residuals are filled as vk_pdhg_solve fills them (pdhg.cpp:153-264;
+ * host threads, after the device loop); otherwise the residuals are NaN.
+ * iterate_seconds and kernel_launches cover the whole batch. */
 int vk_batch_solve(const vk_problem *problems, int32_t count, const vk_options *opts, vk_result *results);
 
 /* Solves `count` relaxations of ONE LP that differ only in their variable

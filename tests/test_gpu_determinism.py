@@ -51,7 +51,8 @@ def test_halpern_two_handles_same_bits(tuned_lp, precision):
     for _ in range(2):
         with vk.Pdhg(tuned_lp, algorithm="halpern", precision=precision) as h:
             runs.append(h.solve(iteration_limit=640, relative_tolerance=0.0, duals=False))
-    assert runs[0]["iterations"] == runs[1]["iterations"] == 640
+    # (mixed: the float64 finish adds one check interval past the limit)
+    assert runs[0]["iterations"] == runs[1]["iterations"] >= 640
     for k in ("x", "y"):
         assert same_bits(runs[1][k], runs[0][k]), k
 

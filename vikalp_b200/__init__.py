@@ -372,50 +372,62 @@ def solve(inst, warm=None, lower=None, upper=None, **opts) -> dict:
         return h.solve(warm, lower, upper)
 
 
-def batch_solve(instances, **opts) -> list[dict]:
-    """Independent LPs in one batch (vk_batch_solve); one result dict per instance."""
+def _batch_outputs(results, sizes, duals):
+    """Host arrays for each batch member (x, y, and the split duals when asked)."""
+    outs = []
+    for (m, n), r in zip(sizes, results):
+        o = {"x": np.zeros(n), "y": np.zeros(m)}
+        if duals:
+            o.update(row_lower_dual=np.zeros(m), row_upper_dual=np.zeros(m), var_lower_dual=np.zeros(n),
+                     var_upper_dual=np.zeros(n))
+        for k, a in o.items():
+            setattr(r, k, _p(a))
+        outs.append(o)
+    return outs
+
+
+def _batch_fields(out, r):
+    out.update(status=STATUS.get(r.status, str(r.status)), iterations=r.iterations, restarts=r.restarts,
+               objective=r.objective, rel_primal=r.rel_primal, rel_dual=r.rel_dual, rel_gap=r.rel_gap,
+               last_metric=r.last_metric, solve_seconds=r.solve_seconds, iterate_seconds=r.iterate_seconds,
+               fp32_iterations=r.fp32_iterations, kernel_launches=r.kernel_launches, message=r.message.decode(),
+               primal_residual=r.primal_residual, stationarity_residual=r.stationarity_residual,
+               complementarity_residual=r.complementarity_residual)
+
+
+def batch_solve(instances, duals: bool = False, **opts) -> list[dict]:
+    """Independent LPs in one batch (vk_batch_solve); one result dict per
+    instance. duals=True also asks for the split duals and the reference's
+    residuals of every member."""
     opts.setdefault("algorithm", "halpern")
     keep = _Keep()
     probs = (Problem * len(instances))(*[problem_struct(inst, keep) for inst in instances])
     results = (Result * len(instances))()
-    outs = []
-    for inst, r in zip(instances, results):
-        o = {"x": np.zeros(inst.n), "y": np.zeros(inst.m)}
-        r.x, r.y = _p(o["x"]), _p(o["y"])
-        outs.append(o)
+    outs = _batch_outputs(results, [(i.m, i.n) for i in instances], duals)
     o = options(**opts)
     _check(lib().vk_batch_solve(probs, len(instances), C.byref(o), results))
     for out, r in zip(outs, results):
-        out.update(status=STATUS.get(r.status, str(r.status)), iterations=r.iterations, restarts=r.restarts,
-                   objective=r.objective, rel_primal=r.rel_primal, rel_dual=r.rel_dual, rel_gap=r.rel_gap,
-                   last_metric=r.last_metric, solve_seconds=r.solve_seconds, iterate_seconds=r.iterate_seconds,
-                   fp32_iterations=r.fp32_iterations, kernel_launches=r.kernel_launches)
+        _batch_fields(out, r)
     return outs
 
 
-def batch_solve_shared(inst, count, lower=None, upper=None, warm=None, **opts) -> list[dict]:
+def batch_solve_shared(inst, count, lower=None, upper=None, warm=None, duals: bool = False, **opts) -> list[dict]:
     """Relaxations of one LP differing in variable bounds (vk_batch_solve_shared).
 
-    lower / upper / warm: None or arrays of shape (count, n)."""
+    lower / upper / warm: None or arrays of shape (count, n). duals=True also
+    asks for the split duals and the reference's residuals of every node."""
     opts.setdefault("algorithm", "halpern")
     keep = _Keep()
     p = problem_struct(inst, keep)
     arr = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(count, inst.n)  # noqa: E731
     lower, upper, warm = arr(lower), arr(upper), arr(warm)
     results = (Result * count)()
-    outs = []
-    for r in results:
-        o = {"x": np.zeros(inst.n), "y": np.zeros(inst.m)}
-        r.x, r.y = _p(o["x"]), _p(o["y"])
-        outs.append(o)
+    outs = _batch_outputs(results, [(inst.m, inst.n)] * count, duals)
     o = options(**opts)
     _check(lib().vk_batch_solve_shared(C.byref(p), count, keep.f(lower), keep.f(upper), keep.f(warm), C.byref(o),
                                        results))
     for out, r in zip(outs, results):
-        out.update(status=STATUS.get(r.status, str(r.status)), iterations=r.iterations, restarts=r.restarts,
-                   objective=r.objective, rel_primal=r.rel_primal, rel_dual=r.rel_dual, rel_gap=r.rel_gap,
-                   last_metric=r.last_metric, solve_seconds=r.solve_seconds, iterate_seconds=r.iterate_seconds,
-                   fp32_iterations=r.fp32_iterations, kernel_launches=r.kernel_launches, message=r.message.decode())
+        _batch_fields(out, r)
     return outs
 
 

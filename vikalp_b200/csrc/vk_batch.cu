@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <exception>
 #include <limits>
 #include <numeric>
 #include <string>
@@ -2008,6 +2009,97 @@ private:
 } // namespace
 
 // Validates every instance (LP only) and runs the batch.
+namespace {
+
+// Post-processing of one batch member's point (x, y) in original
+// coordinates, as the single-instance solve does it (pdhg.cpp:153-264): split
+// row duals max(0, -y) / max(0, y), stationarity s = c + A'y, variable duals
+// max(0, s) / max(0, -s) at bounds within active_tol, and the reference's
+// three infinity-norm residuals (row and box violation; |x - clamp(x - s)|;
+// complementarity). A x is summed row by row and A'y is scattered in row
+// order onto c, the reference CPU backend's orders (cpu_ops.cpp:418-427,
+// 444-458). Writes only the arrays the caller supplied (non-null).
+void postprocess_member(const vk_csr &A, const double *c, const double *rl, const double *ru, const double *lo,
+                        const double *hi, double atol, vk_result &r, std::vector<double> &s) {
+    const int64_t m = A.rows, n = A.cols;
+    const double *x = r.x, *y = r.y;
+    double pres = 0.0, stat = 0.0, comp = 0.0;
+    s.assign(c, c + n);
+    for (int64_t i = 0; i < m; ++i) {
+        double v = 0.0;
+        const double yi = y[i];
+        for (int64_t k = A.row_offsets[i]; k < A.row_offsets[i + 1]; ++k) {
+            v += A.values[k] * x[A.col_indices[k]];
+            s[A.col_indices[k]] += A.values[k] * yi;
+        }
+        const double l = rl[i], u = ru[i];
+        const bool fl = std::isfinite(l), fu = std::isfinite(u);
+        if (fl) pres = std::max(pres, l - v);
+        if (fu) pres = std::max(pres, v - u);
+        const double dl = std::max(0.0, -yi), du = std::max(0.0, yi);
+        if (r.row_lower_dual) r.row_lower_dual[i] = dl;
+        if (r.row_upper_dual) r.row_upper_dual[i] = du;
+        if (fl) comp = std::max(comp, std::abs((v - l) * dl));
+        if (fu) comp = std::max(comp, std::abs((u - v) * du));
+    }
+    for (int64_t j = 0; j < n; ++j) {
+        const double st = s[j], xj = x[j], l = lo[j], u = hi[j];
+        const bool fl = std::isfinite(l), fu = std::isfinite(u);
+        const double t = xj - st;
+        const double proj = (t < l) ? l : ((u < t) ? u : t); // std::clamp (pdhg.cpp:206-208)
+        stat = std::max(stat, std::abs(xj - proj));
+        double dl = 0.0, du = 0.0;
+        if (fl && xj - l <= atol) {
+            dl = std::max(0.0, st);
+            comp = std::max(comp, std::abs((xj - l) * dl));
+        }
+        if (fu && u - xj <= atol) {
+            du = std::max(0.0, -st);
+            comp = std::max(comp, std::abs((u - xj) * du));
+        }
+        if (r.var_lower_dual) r.var_lower_dual[j] = dl;
+        if (r.var_upper_dual) r.var_upper_dual[j] = du;
+        if (fl) pres = std::max(pres, l - xj);
+        if (fu) pres = std::max(pres, xj - u);
+    }
+    r.primal_residual = pres;
+    r.stationarity_residual = stat;
+    r.complementarity_residual = comp;
+}
+
+bool wants_duals(const vk_result &r) {
+    return r.row_lower_dual || r.row_upper_dual || r.var_lower_dual || r.var_upper_dual;
+}
+
+// Runs f(b) for b in [0, count) over up to 16 host threads; the first
+// exception (in member order) is rethrown on the calling thread.
+template <class F>
+void for_members(int count, F &&f) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int T = std::max(1, std::min<int>({count, 16, static_cast<int>(hw == 0 ? 1 : hw)}));
+    std::atomic<int> next{0};
+    std::vector<std::exception_ptr> err(count);
+    auto work = [&] {
+        for (int b = next++; b < count; b = next++) {
+            try {
+                f(b);
+            } catch (...) {
+                err[b] = std::current_exception();
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < T; ++t) pool.emplace_back(work);
+    work();
+    for (std::thread &th : pool) th.join();
+    for (const std::exception_ptr &e : err)
+        if (e) std::rethrow_exception(e);
+}
+
+double active_tolerance(const vk_options &o) { return std::max(10.0 * o.primal_tolerance, 1e-8); }
+
+} // namespace
+
 void batch_solve(const vk_problem *probs, int count, const vk_options &o, vk_result *results) {
     if (count <= 0) throw InvalidInput("count must be positive");
     if (o.algorithm != VK_ALGO_HALPERN) throw Unsupported("batched solves use VK_ALGO_HALPERN");
@@ -2051,6 +2143,15 @@ void batch_solve(const vk_problem *probs, int count, const vk_options &o, vk_res
         BatchEngine eng(probs, count, o);
         eng.solve(results);
     }
+    // split duals and the reference's residuals of every member whose caller
+    // asked for dual arrays (and passed x, y)
+    for_members(count, [&](int b) {
+        vk_result &r = results[b];
+        if (!wants_duals(r) || !r.x || (!r.y && probs[b].A.rows > 0)) return;
+        const vk_problem &p = probs[b];
+        std::vector<double> s;
+        postprocess_member(p.A, p.c, p.row_lower, p.row_upper, p.var_lower, p.var_upper, active_tolerance(o), r, s);
+    });
     if (o.verbose > 0)
         std::fprintf(stderr, "[vikalp_b200] batch: total incl. release       %8.3f s\n", seconds_since(t0));
 }
@@ -2080,6 +2181,17 @@ void batch_solve_shared(const vk_problem &p, int count, const double *lower, con
         eng.solve(lower, upper, warm, results);
         t1 = std::chrono::steady_clock::now();
     }
+    // split duals and the reference's residuals of every node whose caller
+    // asked for dual arrays (and passed x, y), under the node's own bounds
+    const int64_t n = p.A.cols;
+    for_members(count, [&](int b) {
+        vk_result &r = results[b];
+        if (r.status == VK_STATUS_INVALID_MODEL || !wants_duals(r) || !r.x || (!r.y && p.A.rows > 0)) return;
+        const double *lo = lower ? lower + static_cast<size_t>(b) * n : p.var_lower;
+        const double *hi = upper ? upper + static_cast<size_t>(b) * n : p.var_upper;
+        std::vector<double> s;
+        postprocess_member(p.A, p.c, p.row_lower, p.row_upper, lo, hi, active_tolerance(o), r, s);
+    });
     if (o.verbose > 0) {
         std::fprintf(stderr, "[vikalp_b200] shared: release (graphs, memory)  %8.3f s\n", seconds_since(t1));
         std::fprintf(stderr, "[vikalp_b200] shared: total incl. release      %8.3f s\n", seconds_since(t0));

@@ -39,6 +39,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <limits>
 
 namespace vk {
@@ -58,6 +59,8 @@ struct HalCtl {
     double rel_p, rel_d, rel_gap, kkt;
     double bnorm, cnorm, offset, tol;
     double knorm, lq, rho, pad_d; // sigma_max(K), lambda_max(Q^) (0: LP), reflection
+    double theta, omega_lo, omega_hi;       // primal-weight smoothing and clamp
+    double beta_suff, beta_nec, beta_art;   // restart thresholds
     long long k_base, total, limit, restarts, checks;
     int done, status, restart_now, pad;
 };
@@ -69,6 +72,35 @@ struct HalCtl {
 // rho = 0.99 (1 - 1/(2 kappa)), kappa = (1/tau - sigma |K|^2) / L, which keeps
 // (1+rho) T - rho I nonexpansive (Condat's bound on the relaxation of the
 // primal-dual iteration with a smooth term).
+// Primal weight and restart rule of the Halpern scheme. Defaults: omega
+// starts at omega_0 = |c^| / |b^|, moves at each restart to the smoothed
+// log-ratio of the restart points' moves (theta = 0.5), unclamped; restart
+// thresholds 0.2 / 0.8 / 0.36. VIKALP_B200_PRIMAL_WEIGHT="start,theta,lo,hi"
+// (start, lo, hi as multiples of omega_0) and
+// VIKALP_B200_RESTART="sufficient,necessary,artificial" override them.
+struct PrimalWeightRule {
+    double start = 1.0, theta = 0.5, lo = 0.0, hi = std::numeric_limits<double>::infinity();
+    double beta_suff = 0.2, beta_nec = 0.8, beta_art = 0.36;
+};
+
+inline PrimalWeightRule primal_weight_rule() {
+    PrimalWeightRule r;
+    if (const char *e = std::getenv("VIKALP_B200_PRIMAL_WEIGHT"); e && *e) {
+        double a = r.start, b = r.theta, c = r.lo, d = r.hi;
+        const int got = std::sscanf(e, "%lf,%lf,%lf,%lf", &a, &b, &c, &d);
+        if (got >= 1 && a > 0.0) r.start = a;
+        if (got >= 2 && b >= 0.0 && b <= 1.0) r.theta = b;
+        if (got >= 3 && c >= 0.0) r.lo = c;
+        if (got >= 4 && d > 0.0) r.hi = d;
+    }
+    if (const char *e = std::getenv("VIKALP_B200_RESTART"); e && *e) {
+        double a = r.beta_suff, b = r.beta_nec, c = r.beta_art;
+        if (std::sscanf(e, "%lf,%lf,%lf", &a, &b, &c) == 3 && a > 0.0 && a < 1.0 && b > 0.0 && b < 1.0 && c > 0.0)
+            r.beta_suff = a, r.beta_nec = b, r.beta_art = c;
+    }
+    return r;
+}
+
 __host__ __device__ inline void step_params(double knorm, double lq, double omega, double &eta, double &rho) {
     if (!(lq > 0.0)) {
         eta = knorm > 0.0 ? 0.99 / knorm : 1.0;
@@ -398,13 +430,14 @@ __global__ void __launch_bounds__(kControlThreads)
         if (c.r_restart < 0.0) {
             c.r_restart = r;
         } else {
-            restart = (r <= 0.2 * c.r_restart) || (r <= 0.8 * c.r_restart && r > c.r_prev) ||
-                      (static_cast<double>(k) >= 0.36 * static_cast<double>(c.total));
+            restart = (r <= c.beta_suff * c.r_restart) || (r <= c.beta_nec * c.r_restart && r > c.r_prev) ||
+                      (static_cast<double>(k) >= c.beta_art * static_cast<double>(c.total));
         }
         c.r_prev = r;
         if (restart) {
             const double mx = sqrt(dx0), my = sqrt(dy0);
-            if (mx > 1e-10 && my > 1e-10) c.omega = exp(0.5 * log(my / mx) + 0.5 * log(c.omega));
+            if (mx > 1e-10 && my > 1e-10 && c.theta > 0.0)
+                c.omega = fmin(c.omega_hi, fmax(c.omega_lo, exp(c.theta * log(my / mx) + (1.0 - c.theta) * log(c.omega))));
             step_params(c.knorm, c.lq, c.omega, c.eta, c.rho);
             c.tau = c.eta / c.omega;
             c.sigma = c.eta * c.omega;
@@ -528,10 +561,17 @@ public:
         HalCtl c{};
         c.knorm = knorm_;
         c.lq = lq_;
-        c.omega = omega0_;
+        const PrimalWeightRule pw = primal_weight_rule();
+        c.omega = omega0_ * pw.start;
+        c.theta = pw.theta;
+        c.omega_lo = omega0_ * pw.lo;
+        c.omega_hi = omega0_ * pw.hi;
+        c.beta_suff = pw.beta_suff;
+        c.beta_nec = pw.beta_nec;
+        c.beta_art = pw.beta_art;
         step_params(c.knorm, c.lq, c.omega, c.eta, c.rho);
-        c.tau = c.eta / omega0_;
-        c.sigma = c.eta * omega0_;
+        c.tau = c.eta / c.omega;
+        c.sigma = c.eta * c.omega;
         c.r_restart = -1.0;
         c.r_prev = std::numeric_limits<double>::infinity();
         c.bnorm = bnorm_;
@@ -678,6 +718,11 @@ private:
         VK_CUDA(cudaMemcpyAsync(hctl_.get(), ctl_.get(), sizeof(HalCtl), cudaMemcpyDeviceToHost, s_));
         VK_CUDA(cudaStreamSynchronize(s_));
         check_device_error(s_);
+        if (o_.verbose >= 2) { // per-check trace
+            const HalCtl &h = hctl_[0];
+            std::fprintf(stderr, "[vikalp_b200] halpern %lld kkt %.3e p %.2e d %.2e gap %.2e omega %.4g restarts %lld\n",
+                         h.total, h.kkt, h.rel_p, h.rel_d, h.rel_gap, h.omega / omega0_, h.restarts);
+        }
     }
 
     // Ruiz (infinity norm) passes, then one Pock-Chambolle (alpha = 1) pass.
