@@ -15,8 +15,9 @@ replicas, no collective on the path). The same line carries:
   e2e            the same metric through the C ABI from host arrays (model
                  upload, device setup, iterations, results copied back)
   halpern        iterations/s of the restarted Halpern scheme, fp64 and mixed
-  time_to_tol    time and iterations to 1e-6 relative KKT (small LP and, with
-                 --ttt, the large LP), fp64 vs mixed
+  time_to_tol    time and iterations to 1e-6 relative KKT, fp64 vs mixed, on
+                 the small LP and on the bench's large LP (its points
+                 re-evaluated by the C oracle; --no-ttt skips the large LP)
   spmv           GB/s of the sparse product kernel, A x and A'y, fp64 / fp32
   batched        768 LPs (512 shared-matrix node relaxations + 256 independent
                  LPs) to 1e-6 relative KKT in two batches, mixed and fp64, vs
@@ -108,13 +109,16 @@ class ClockSampler:
 
 def profile_traffic(kernel_name):
     """DRAM bytes per launch of a fused pass (the column or the row pass of the
-    reference-scheme iteration on the large LP) from its committed ncu summary."""
+    reference-scheme iteration on the large LP) from its committed ncu summary,
+    with the kernel variant that capture pinned: (bytes, variant, file)."""
     name = "col_pass_large_lp.md" if kernel_name.startswith("column") else "row_pass_large_lp.md"
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
-        return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
-    return float(m.group(1)) if m else None
+        return None, None, name
+    text = open(p).read()
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", text)
+    v = re.search(r"Kernel: variant (\d+)", text)
+    return (float(m.group(1)) if m else None), (int(v.group(1)) if v else None), name
 
 
 def spmv_figures(inst, torch, stream):
@@ -149,16 +153,29 @@ def spmv_figures(inst, torch, stream):
     return out
 
 
-def time_to_tolerance(inst, label, limit, time_limit=float("inf")):
+def time_to_tolerance(inst, label, limit, time_limit=float("inf"), check=False):
+    """Both precisions of the Halpern scheme to 1e-6 relative KKT. With check,
+    the returned point's relative KKT is evaluated again by the C oracle (the
+    checker, not the thing timed) and the mixed answer's error against the
+    float64 answer is reported."""
     import vikalp_b200 as vk
-    res = {}
+    res, pts = {}, {}
     for prec in ("fp64", "mixed"):
         with vk.Pdhg(inst, algorithm="halpern", precision=prec, iteration_limit=limit,
                      relative_tolerance=1e-6, time_limit_seconds=time_limit) as h:
             r = h.solve(duals=False)
+        pts[prec] = r
         res[prec] = {"status": r["status"], "iterations": r["iterations"], "fp32_iterations": r["fp32_iterations"],
                      "iterate_s": round(r["iterate_seconds"], 4), "solve_s": round(r["solve_seconds"], 4),
                      "rel_kkt": max(r["rel_primal"], r["rel_dual"], r["rel_gap"]), "objective": r["objective"]}
+        if check:
+            from oracle.oracle import Oracle
+            k = Oracle().rel_kkt(inst, r["x"], r["y"])
+            res[prec]["rel_kkt_by_c_oracle"] = max(k["rel_primal"], k["rel_dual"], k["rel_gap"])
+    f64, mx = pts["fp64"], pts["mixed"]
+    res["mixed_vs_fp64"] = {
+        "objective_rel_diff": abs(mx["objective"] - f64["objective"]) / (1 + abs(f64["objective"])),
+        "x_rel_diff": float(np.linalg.norm(mx["x"] - f64["x"]) / max(np.linalg.norm(f64["x"]), 1e-300))}
     f, mx = res["fp64"], res["mixed"]
     if f["status"] == "Optimal" and mx["status"] == "Optimal":
         res["mixed_speedup_vs_fp64"] = round(f["iterate_s"] / mx["iterate_s"], 3)
@@ -166,16 +183,16 @@ def time_to_tolerance(inst, label, limit, time_limit=float("inf")):
     return res
 
 
-def batched_figures(sample_every=64):
+def batched_figures():
     """The batched workload: 512 node relaxations of one LP (m=50,000, n=100,000,
     6 nonzeros per column, 1-12 tightened variables each) and 256 independent
     LPs (m log-uniform on [500, 20000], n=2m, 8 per column), all to 1e-6
-    relative KKT. The two batches run one after the other; wall time from
-    host arrays to results. The plain-FP64 comparison solves
-    instances one by one with the single-instance float64 engine (a resident
-    model for the nodes, create+solve for each independent LP) on a systematic
-    sample (every `sample_every`-th node, every (sample_every/2)-th LP) and
-    scales the sample's mean to the whole set."""
+    relative KKT. Batched: one vk_batch_solve_together call (both batches set up,
+    then both device loops in flight on their own streams); wall time from host
+    arrays to results. Also timed: the two batches one after the other, and the
+    plain-FP64 comparison, which solves every one of the 768 instances one by
+    one with the single-instance float64 engine (a resident model for the
+    nodes, create + solve for each independent LP)."""
     import vikalp_b200 as vk
     from vikalp_b200 import synthetic
     node_lp = synthetic.lp_uniform(50000, 100000, 6, seed=2025)
@@ -183,66 +200,58 @@ def batched_figures(sample_every=64):
     indep = synthetic.workload_independent_lps(256)
     tol = dict(iteration_limit=200000, relative_tolerance=1e-6, time_limit_seconds=300)
 
-    def run(prec):
-        res = {}
-
-        def shared():
-            t = time.perf_counter()
-            res["shared"] = vk.batch_solve_shared(node_lp, 512, lo, hi, precision=prec, **tol)
-            res["shared_s"] = time.perf_counter() - t
-
-        def independent():
-            t = time.perf_counter()
-            res["indep"] = vk.batch_solve(indep, precision=prec, **tol)
-            res["indep_s"] = time.perf_counter() - t
-
-        # one after the other: run concurrently, each batch's setup (device
-        # allocation and release) waits on the other's iterations
-        t0 = time.perf_counter()
-        shared()
-        independent()
-        wall = time.perf_counter() - t0
-        rs = res["shared"] + res["indep"]
+    def summary(rs, wall):
         status = {}
         for r in rs:
             status[r["status"]] = status.get(r["status"], 0) + 1
-        return {"wall_s": round(wall, 3), "shared_s": round(res["shared_s"], 3), "independent_s": round(res["indep_s"], 3),
-                "shared_iterate_s": round(res["shared"][0]["iterate_seconds"], 3),
-                "independent_iterate_s": round(res["indep"][0]["iterate_seconds"], 3),
-                "status": status, "max_iterations": int(max(r["iterations"] for r in rs)),
+        return {"wall_s": round(wall, 3), "status": status, "max_iterations": int(max(r["iterations"] for r in rs)),
                 "max_rel_kkt": float(max(max(r["rel_primal"], r["rel_dual"], r["rel_gap"]) for r in rs))}
+
+    def together(prec):
+        t0 = time.perf_counter()
+        nodes, lps = vk.batch_solve_together(node_lp, 512, indep, lo, hi, precision=prec, **tol)
+        out = summary(nodes + lps, time.perf_counter() - t0)
+        out["shared_iterate_s"] = round(nodes[0]["iterate_seconds"], 3)
+        out["independent_iterate_s"] = round(lps[0]["iterate_seconds"], 3)
+        return out
+
+    def one_after_other(prec):
+        t0 = time.perf_counter()
+        nodes = vk.batch_solve_shared(node_lp, 512, lo, hi, precision=prec, **tol)
+        t1 = time.perf_counter()
+        lps = vk.batch_solve(indep, precision=prec, **tol)
+        out = summary(nodes + lps, time.perf_counter() - t0)
+        out.update(shared_s=round(t1 - t0, 3), independent_s=round(time.perf_counter() - t1, 3))
+        return out
 
     out = {"workload": "512 node LPs sharing A (m=5e4 n=1e5 nnz=600k, 1-12 tightened bounds) + 256 independent LPs "
                        "(m log-uniform 500..20000, n=2m, 8/col; 19.7M nnz), to 1e-6 relative KKT",
-           "mixed": run("mixed"), "fp64_batched": run("fp64")}
-    # plain float64, one instance at a time (sample)
-    # each sampled instance is solved twice and keeps the faster time, so a
-    # stall of the host in one of the two runs does not enter the estimate
-    node_t, indep_t = [], []
-
-    def best_of_two(run):
-        ts = []
-        for _ in range(2):
-            t = time.perf_counter()
-            r = run()
-            ts.append(time.perf_counter() - t)
-            assert r["status"] == "Optimal", r["status"]
-        return min(ts)
-
+           "mixed": together("mixed"), "fp64_batched": together("fp64"),
+           "mixed_one_batch_after_the_other": one_after_other("mixed")}
+    # plain float64, every instance one by one
+    # (one untimed solve of each kind first, so no one-time cost of the path enters)
+    node_t, indep_t, statuses = [], [], {}
     with vk.Pdhg(node_lp, algorithm="halpern", precision="fp64", **tol) as h:
-        for b in range(0, 512, sample_every):
-            node_t.append(best_of_two(lambda: h.solve(lower=lo[b], upper=hi[b], duals=False)))
-    # one untimed create + solve first (an instance outside the sample), so the
-    # first sample carries no one-time cost of the path
-    vk.solve(indep[1], algorithm="halpern", precision="fp64", **tol)
-    for b in range(0, 256, sample_every // 2):
-        indep_t.append(best_of_two(lambda: vk.solve(indep[b], algorithm="halpern", precision="fp64", **tol)))
-    est = 512 * statistics.mean(node_t) + 256 * statistics.mean(indep_t)
-    out["plain_fp64_one_by_one"] = {"estimated_s": round(est, 3), "node_sample_s": [round(t, 4) for t in node_t],
-                                    "independent_sample_s": [round(t, 4) for t in indep_t],
-                                    "sample": f"{len(node_t)} of 512 nodes, {len(indep_t)} of 256 LPs, each the faster of two solves; "
-                                                                          "mean x count"}
-    out["speedup_mixed_batched_vs_plain_fp64"] = round(est / out["mixed"]["wall_s"], 2)
+        h.solve(lower=lo[0], upper=hi[0], duals=False)
+        t_all = time.perf_counter()
+        for b in range(512):
+            t = time.perf_counter()
+            r = h.solve(lower=lo[b], upper=hi[b], duals=False)
+            node_t.append(time.perf_counter() - t)
+            statuses[r["status"]] = statuses.get(r["status"], 0) + 1
+    vk.solve(indep[0], algorithm="halpern", precision="fp64", **tol)
+    for inst in indep:
+        t = time.perf_counter()
+        r = vk.solve(inst, algorithm="halpern", precision="fp64", **tol)
+        indep_t.append(time.perf_counter() - t)
+        statuses[r["status"]] = statuses.get(r["status"], 0) + 1
+    measured = sum(node_t) + sum(indep_t)
+    out["plain_fp64_one_by_one"] = {"measured_s": round(measured, 3), "nodes_s": round(sum(node_t), 3),
+                                    "independent_s": round(sum(indep_t), 3), "status": statuses,
+                                    "instances": len(node_t) + len(indep_t),
+                                    "slowest_node_s": round(max(node_t), 4),
+                                    "slowest_independent_s": round(max(indep_t), 4)}
+    out["speedup_mixed_batched_vs_plain_fp64"] = round(measured / out["mixed"]["wall_s"], 2)
     return out
 
 
@@ -316,6 +325,41 @@ def reference_cpu_rate(inst, budget_s, warmup=3):
     return iters / secs, iters, secs
 
 
+def reference_cpu_end_to_end(small_budget_s=20.0, each_budget_s=8.0):
+    """The reference's own end-to-end CPU solve, vikalp::solve(model, options)
+    with the default backend preference (its CPU backend, oracle/_ref compiled
+    from its sources), on the small LP and on bounded samples of the other
+    LP workloads: 4 of the 256 differentiable-workload LPs and 4 of the 256
+    independent LPs of the batched workload (sizes spread over the range).
+    Each run stops at the reference's own tolerance (1e-6 absolute residuals)
+    or at its time budget; the returned point's relative KKT is evaluated by
+    the C oracle (the checker). Baseline only."""
+    from oracle.oracle import Oracle
+    from oracle.oracle import Reference
+    from vikalp_b200 import synthetic
+    ref, orc = Reference(), Oracle()
+
+    def one(inst, budget):
+        t = time.perf_counter()
+        r = ref.solve(inst, iteration_limit=10_000_000, time_limit_seconds=budget, primal_tolerance=1e-6,
+                      dual_tolerance=1e-6)
+        secs = time.perf_counter() - t
+        k = orc.rel_kkt(inst, r["x"], r["y"])
+        return {"status": r["status"], "iterations": r["iterations"], "seconds": round(secs, 2),
+                "rel_kkt": max(k["rel_primal"], k["rel_dual"], k["rel_gap"]), "backend": r["backend"]}
+
+    out = {"small_lp": one(synthetic.workload_small_lp(), small_budget_s)}
+    adj = [synthetic.lp_uniform(1000, 2000, 8, seed=7000 + s) for s in (0, 85, 170, 255)]
+    out["adjoint_lps_sample"] = [one(i, each_budget_s) for i in adj]
+    indep = synthetic.workload_independent_lps(256)
+    order = sorted(range(256), key=lambda i: indep[i].m)
+    out["independent_lps_sample"] = [dict(one(indep[i], each_budget_s), m=indep[i].m) for i in
+                                     (order[0], order[85], order[170], order[255])]
+    out["note"] = (f"1 core; per-instance budget {small_budget_s:.0f} s (small LP) / {each_budget_s:.0f} s "
+                   "(samples); the reference stops on its absolute 1e-6 residuals")
+    return out
+
+
 def reference_cpu_steps(inst, steps, warmup, budget_s):
     """The reference arm's timing: `warmup` untimed then `steps` timed steps of
     the reference's own CPU PDHG iteration (pdhg.cpp:92-130 call sequence through
@@ -341,8 +385,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--ttt", action="store_true", help="also time the large LP to 1e-6 relative KKT")
-    ap.add_argument("--ttt-seconds", type=float, default=60.0, help="time cap per precision for --ttt")
+    ap.add_argument("--no-ttt", action="store_true", help="skip timing the large LP to 1e-6 relative KKT")
+    ap.add_argument("--ttt-seconds", type=float, default=120.0, help="time cap per precision for the large LP")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-workload figures")
     ap.add_argument("--profile-spmv", choices=["fp64", "fp32"], default=None,
@@ -422,12 +466,14 @@ def main():
     # five calls (each: create with upload and device setup, solve, results
     # back); the median is reported: the host side (page faults of fresh
     # result arrays, driver allocations) varies from call to call
-    runs = []
+    runs, creates = [], []
     for _ in range(5):
         replicas.barrier(ranks)
         t0 = time.perf_counter()
-        r2 = vk.solve(inst, algorithm="reference", iteration_limit=K * CHUNK, primal_tolerance=0.0,
-                      dual_tolerance=0.0)
+        with vk.Pdhg(inst, algorithm="reference", iteration_limit=K * CHUNK, primal_tolerance=0.0,
+                     dual_tolerance=0.0) as he:
+            creates.append(time.perf_counter() - t0)
+            r2 = he.solve()
         torch.cuda.synchronize()
         runs.append(replicas.whole_job_rate(ranks, r2["iterations"], time.perf_counter() - t0))
     e2e_rate, t_e2e = sorted(runs)[len(runs) // 2]
@@ -438,6 +484,7 @@ def main():
     e2e = {"value": round(e2e_rate, 3), "unit": "iter/s",
            "h2d_bytes_per_step": int(h2d / steps_e2e), "d2h_bytes_per_step": int(d2h / steps_e2e),
            "seconds": round(t_e2e, 3), "runs_seconds": [round(t, 3) for _, t in runs],
+           "create_seconds": [round(t, 3) for t in creates],
            "note": "create (upload + device setup) + solve + results, pageable host arrays; median of 5 calls"}
     line = {"metric": METRIC, "value": round(value, 3), "unit": "iter/s", "n_gpus": ws, "steps": iters // CHUNK,
             "warmup": W, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True, "scaling": "weak",
@@ -448,8 +495,15 @@ def main():
         total = sum(p["ms"] * p["launches"] for p in prof)
         dom = max(prof, key=lambda p: p["ms"] * p["launches"])
         achieved = dom["bytes"] / (dom["ms"] * 1e-3) / 1e9
+        traffic, cap_variant, cap_file = profile_traffic(dom["name"])
+        live = re.search(r"variant (\d+)", dom["name"])
+        live_variant = int(live.group(1)) if live else None
         line["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                            "frac": round(achieved / peak, 4), "traffic": profile_traffic(dom["name"]),
+                            "frac": round(achieved / peak, 4), "traffic": traffic,
+                            "traffic_source": f"ncu capture committed in profiles/{cap_file} (kernel variant "
+                                              f"{cap_variant}); the timed run's pass ran variant {live_variant}"
+                                              + ("" if cap_variant == live_variant else
+                                                 " (a different variant: the capture's bytes are indicative)"),
                             "kernel": f"{dom['name']} of the reference-scheme iteration (fp64, FAST order)",
                             "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                             "algorithmic_bytes": int(dom["bytes"]), "ms": round(dom["ms"], 4),
@@ -471,8 +525,9 @@ def main():
         line["halpern"] = hal
         small = synthetic.workload_small_lp()
         ttt = {"small_lp": time_to_tolerance(small, "lp m=2000 n=5000 nnz=40000", 400000)}
-        if args.ttt:
-            ttt["large_lp"] = time_to_tolerance(inst, "large lp", 2_000_000, time_limit=args.ttt_seconds)
+        if not args.no_ttt:
+            ttt["large_lp"] = time_to_tolerance(inst, "lp m=1e6 n=2e6 nnz=21.1M (the bench's LP)", 2_000_000,
+                                                time_limit=args.ttt_seconds, check=True)
         line["time_to_tol"] = ttt
         if not args.no_batched:
             line["batched"] = batched_figures()
@@ -481,6 +536,7 @@ def main():
                                                           400000, time_limit=120)
         line["reference_cuda"] = reference_cuda_rate(inst)
         if ws == 1:
+            line["cpu_reference_end_to_end"] = reference_cpu_end_to_end()
             rate, n_it, secs = reference_cpu_rate(inst, budget_s=20.0)
             line["cpu_baseline"] = {"value": round(rate, 4), "unit": "iter/s", "cores": 1, "kind": "reference",
                                     "sample": f"{n_it} iterations of the reference's pdhg.cpp:92-130 call sequence "

@@ -325,6 +325,19 @@ int vk_batch_solve(const vk_problem *problems, int32_t count, const vk_options *
 int vk_batch_solve_shared(const vk_problem *problem, int32_t count, const double *lower, const double *upper,
                           const double *warm, const vk_options *opts, vk_result *results);
 
+/* vk_batch_solve_shared(problem, node_count, lower, upper, warm, ...) and
+ * vk_batch_solve(problems, count, ...) in one call, the two device loops in
+ * flight together: both batches are set up first, then each iterates on its
+ * own stream from its own host thread, so neither waits for the other's
+ * iterations and the GPU is shared between them. node_results[b] and
+ * results[b] are what the two calls would return (each member keeps its own
+ * primal weight, restarts and stopping). The mixed workload of a
+ * branch-and-bound run that also solves independent LPs; no counterpart in the
+ * reference (it solves one LP at a time, BranchAndBound.cpp:296-297). */
+int vk_batch_solve_together(const vk_problem *problem, int32_t node_count, const double *lower,
+                            const double *upper, const double *warm, const vk_problem *problems, int32_t count,
+                            const vk_options *opts, vk_result *node_results, vk_result *results);
+
 /* ---- differentiation ---------------------------------------------------------- */
 
 typedef struct {

@@ -11,7 +11,7 @@ pdhg.cpp:133-145). It follows the same definitions, float64 throughout:
   Halpern update with lambda = (k+1)/(k+2);
 * every `check_every` iterations: relative KKT of (x^, y^) in original units,
   stop at `tol`, restart rule on the fixed-point residual, primal weight
-  update on restart.
+  update on restart (OMEGA_START, THETA, RESTART below: the library's rule).
 
 Used by tests/ and the bench's CPU baseline only.
 """
@@ -136,9 +136,25 @@ def rel_kkt(inst, x, y, lower=None, upper=None):
                 rel_gap=abs(pobj - dobj) / (1 + abs(pobj) + abs(dobj)), primal_objective=pobj, dual_objective=dobj)
 
 
+# The library's default primal-weight / restart rule (PrimalWeightRule,
+# vk_engine.cuh): omega starts at OMEGA_START x |c^| / |b^|, is smoothed with
+# THETA at each restart, restart thresholds RESTART = (sufficient, necessary,
+# artificial).
+OMEGA_START = 1.0
+THETA = 0.5
+FREEZE = 0.0  # no primal-weight update once the relative KKT error is below this
+RESTART = (0.2, 0.8, 0.36)
+
+
 def solve(inst, tol=1e-6, iteration_limit=100000, check_every=64, rho=None, warm=None, lower=None, upper=None,
-          trace=False, theta=0.5, omega0=None):
-    """rho: reflection override (default: step_params' choice, 1 for an LP)."""
+          trace=False, theta=None, omega0=None, omega_start=None, restart=None, freeze=None):
+    """rho: reflection override (default: step_params' choice, 1 for an LP).
+    theta / omega_start / restart: the rule (defaults: THETA, OMEGA_START,
+    RESTART); omega0 replaces the starting primal weight outright."""
+    theta = THETA if theta is None else theta
+    freeze = FREEZE if freeze is None else freeze
+    omega_start = OMEGA_START if omega_start is None else omega_start
+    b_suff, b_nec, b_art = RESTART if restart is None else restart
     A = _csr(inst)
     Q = _q(inst)
     m, n = A.shape
@@ -159,6 +175,7 @@ def solve(inst, tol=1e-6, iteration_limit=100000, check_every=64, rho=None, warm
     bnorm, cnorm = np.linalg.norm(b_orig), np.linalg.norm(inst.c)
     cs2, bs2 = np.sum(c * c), np.sum((b_orig * r) ** 2)
     omega = np.sqrt(cs2) / np.sqrt(bs2) if (cs2 > 1e-20 and bs2 > 1e-20) else 1.0
+    omega *= omega_start
     if omega0 is not None:
         omega = omega0
     smax = sigma_max(K) if K.nnz else 0.0
@@ -203,11 +220,11 @@ def solve(inst, tol=1e-6, iteration_limit=100000, check_every=64, rho=None, warm
         if r_restart < 0:
             r_restart = rr
         else:
-            restart = rr <= 0.2 * r_restart or (rr <= 0.8 * r_restart and rr > r_prev) or k >= 0.36 * total
+            restart = rr <= b_suff * r_restart or (rr <= b_nec * r_restart and rr > r_prev) or k >= b_art * total
         r_prev = rr
         if restart:
             mx, my = np.sqrt(dx0), np.sqrt(dy0)
-            if mx > 1e-10 and my > 1e-10:
+            if mx > 1e-10 and my > 1e-10 and theta > 0 and kkt >= freeze:
                 omega = np.exp(theta * np.log(my / mx) + (1 - theta) * np.log(omega))
             eta, rho_k = step_params(smax, lq, omega)
             rho_k = rho_k if rho is None else rho

@@ -58,7 +58,7 @@ vikalp::Model small_lp(int m, int n, uint64_t seed) {
     vikalp::Model md;
     md.constraint_matrix.pattern.rows = m;
     md.constraint_matrix.pattern.columns = n;
-    md.constraint_matrix.pattern.row_offsets.push_back(0);
+    md.constraint_matrix.pattern.row_offsets.assign(1, 0); // CsrPattern starts as {0}
     for (auto &row : rows) {
         std::sort(row.begin(), row.end());
         for (auto &[c, v] : row) {
@@ -99,6 +99,7 @@ vikalp::SolverOptions options() {
 
 void cpu_routes() {
     const auto model = small_lp(20, 40, 3);
+    expect(model.validate().empty(), "test model valid");
     vikalp::BatchedRelaxationOracle oracle;
     expect(oracle.solve_batch(model, {}, options()).empty(), "empty batch: no results");
     // the CPU backend is not in this library: every node says so, in order
@@ -175,6 +176,7 @@ std::vector<std::tuple<int, double, int>> batched_loop(const vikalp::Model &mode
 void gpu_batches() {
     const int m = 40, n = 100;
     const auto model = small_lp(m, n, 11);
+    expect(model.validate().empty(), "test model valid");
     vikalp::BatchedRelaxationOracle batched;
     vikalp::CudaRelaxationOracle one;
     // 10 nodes: tightened bounds, a warm start, a wrong-size override, a crossed interval

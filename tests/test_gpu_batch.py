@@ -14,6 +14,7 @@
 
 import numpy as np
 import pytest
+import scipy.sparse as sp
 
 import vikalp_b200 as vk
 from oracle import halpern
@@ -184,3 +185,62 @@ def test_shared_invalid_member_and_warm_start(node_lp):
         assert again[b]["restarts"] == want["restarts"]
         for k in ("x", "y"):
             assert np.max(np.abs(again[b][k] - want[k])) <= 1e-8 * (1.0 + np.abs(want[k]).max()), (b, k)
+
+
+# ---- duals and residuals of batch members -----------------------------------------
+
+
+def _post_reference(inst, x, y, lo, hi, atol=1e-6):
+    """The post-processing of pdhg.cpp:153-264 in numpy (split row duals, variable
+    duals at bounds within active_tol, the three infinity-norm residuals)."""
+    A = sp.csr_matrix((inst.values, inst.col_idx, inst.row_offsets), shape=(inst.m, inst.n))
+    ax = A @ x
+    rl, ru = inst.row_lower, inst.row_upper
+    ld, ud = np.maximum(0, -y), np.maximum(0, y)
+    s = inst.c + A.T @ y
+    at_lo = np.isfinite(lo) & (x - lo <= atol)
+    at_hi = np.isfinite(hi) & (hi - x <= atol)
+    vld = np.where(at_lo, np.maximum(0, s), 0.0)
+    vud = np.where(at_hi, np.maximum(0, -s), 0.0)
+    with np.errstate(invalid="ignore"):
+        pres = max(np.max(np.where(np.isfinite(rl), rl - ax, 0), initial=0.0),
+                   np.max(np.where(np.isfinite(ru), ax - ru, 0), initial=0.0),
+                   np.max(np.where(np.isfinite(lo), lo - x, 0), initial=0.0),
+                   np.max(np.where(np.isfinite(hi), x - hi, 0), initial=0.0))
+    stat = np.max(np.abs(x - np.clip(x - s, lo, hi)), initial=0.0)
+    return dict(row_lower_dual=ld, row_upper_dual=ud, var_lower_dual=vld, var_upper_dual=vud,
+                primal_residual=pres, stationarity_residual=stat)
+
+
+def test_batch_members_duals_and_residuals(members, node_lp):
+    # the options' primal tolerance (1e-7) gives active_tol = max(10 * 1e-7, 1e-8) = 1e-6
+    outs = vk.batch_solve(members, duals=True, iteration_limit=200000, relative_tolerance=1e-6)
+    inst, lo, hi = node_lp
+    nodes = vk.batch_solve_shared(inst, len(lo), lo, hi, duals=True, iteration_limit=200000, relative_tolerance=1e-6)
+    cases = [(m, r, m.var_lower, m.var_upper) for m, r in zip(members, outs)]
+    cases += [(inst, r, lo[b], hi[b]) for b, r in enumerate(nodes)]
+    for model, r, l, u in cases:
+        want = _post_reference(model, r["x"], r["y"], l, u)
+        for k in ("row_lower_dual", "row_upper_dual", "var_lower_dual", "var_upper_dual"):
+            assert np.allclose(r[k], want[k], rtol=1e-12, atol=1e-12), k
+        for k in ("primal_residual", "stationarity_residual"):
+            assert abs(r[k] - want[k]) <= 1e-12 * (1 + abs(want[k])), (k, r[k], want[k])
+        assert np.isfinite(r["complementarity_residual"])
+    # without dual arrays the residuals stay NaN
+    plain = vk.batch_solve(members[:2], iteration_limit=200000, relative_tolerance=1e-6)
+    assert np.isnan(plain[0]["primal_residual"])
+
+
+# ---- a node batch and independent LPs in flight together ---------------------------
+
+
+def test_together_equals_the_two_batches(members, node_lp):
+    inst, lo, hi = node_lp
+    opts = dict(precision="mixed", iteration_limit=200000, relative_tolerance=1e-6)
+    nodes, lps = vk.batch_solve_together(inst, len(lo), members, lo, hi, **opts)
+    n_alone = vk.batch_solve_shared(inst, len(lo), lo, hi, **opts)
+    l_alone = vk.batch_solve(members, **opts)
+    for got, want in list(zip(nodes, n_alone)) + list(zip(lps, l_alone)):
+        assert got["status"] == want["status"] == "Optimal"
+        assert got["iterations"] == want["iterations"]
+        assert np.array_equal(got["x"], want["x"]) and np.array_equal(got["y"], want["y"])

@@ -134,6 +134,8 @@ _SIGNATURES = {
     "vk_lp_adjoint": (C.c_int, [C.POINTER(Problem), C.c_int32, _f64p, _f64p, _f64p, C.c_double,
                                 C.POINTER(AdjointOptions), _f64p, _f64p, _f64p, C.POINTER(AdjointInfo)]),
     "vk_diag_bounded_wait": (C.c_int, [C.c_int32]),
+    "vk_batch_solve_together": (C.c_int, [C.POINTER(Problem), C.c_int32, _f64p, _f64p, _f64p, C.POINTER(Problem),
+                                          C.c_int32, C.POINTER(Options), C.POINTER(Result), C.POINTER(Result)]),
 }
 
 # include/vikalp_mps.h: the MPS ingest path, exported by the C++ host layer (libvikalp.so).
@@ -429,6 +431,31 @@ def batch_solve_shared(inst, count, lower=None, upper=None, warm=None, duals: bo
     for out, r in zip(outs, results):
         _batch_fields(out, r)
     return outs
+
+
+def batch_solve_together(inst, count, instances, lower=None, upper=None, warm=None, duals: bool = False,
+                         **opts) -> tuple[list[dict], list[dict]]:
+    """A node batch of `inst` (as batch_solve_shared) and the independent LPs
+    `instances` (as batch_solve) with both device loops in flight at once
+    (vk_batch_solve_together). Returns (node results, instance results)."""
+    opts.setdefault("algorithm", "halpern")
+    keep = _Keep()
+    p = problem_struct(inst, keep)
+    arr = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(count, inst.n)  # noqa: E731
+    lower, upper, warm = arr(lower), arr(upper), arr(warm)
+    probs = (Problem * len(instances))(*[problem_struct(i, keep) for i in instances])
+    nres = (Result * count)()
+    ires = (Result * len(instances))()
+    nouts = _batch_outputs(nres, [(inst.m, inst.n)] * count, duals)
+    iouts = _batch_outputs(ires, [(i.m, i.n) for i in instances], duals)
+    o = options(**opts)
+    _check(lib().vk_batch_solve_together(C.byref(p), count, keep.f(lower), keep.f(upper), keep.f(warm), probs,
+                                         len(instances), C.byref(o), nres, ires))
+    for out, r in zip(nouts, nres):
+        _batch_fields(out, r)
+    for out, r in zip(iouts, ires):
+        _batch_fields(out, r)
+    return nouts, iouts
 
 
 def lp_adjoint(instances, xs, ys, grads, dL_dobj=0.0, **opts) -> list[dict]:

@@ -23,6 +23,7 @@
 #include <limits>
 #include <numeric>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <type_traits>
 
@@ -38,6 +39,7 @@ struct BCtl {
     long long *k_base, *iters, *restarts;
     int *done, *status, *restart_now;
     double tol;
+    double theta, freeze, beta_suff, beta_nec, beta_art; // primal_weight_rule()
     long long limit;
     int count;
 };
@@ -340,14 +342,15 @@ __global__ void batch_control_kernel(BCtl c, const double *cs, const double *rs,
     if (c.r_restart[b] < 0.0) {
         c.r_restart[b] = r;
     } else {
-        restart = (r <= 0.2 * c.r_restart[b]) || (r <= 0.8 * c.r_restart[b] && r > c.r_prev[b]) ||
-                  (static_cast<double>(k) >= 0.36 * static_cast<double>(c.iters[b]));
+        restart = (r <= c.beta_suff * c.r_restart[b]) || (r <= c.beta_nec * c.r_restart[b] && r > c.r_prev[b]) ||
+                  (static_cast<double>(k) >= c.beta_art * static_cast<double>(c.iters[b]));
     }
     c.r_prev[b] = r;
     if (restart) {
         const double mx = sqrt(dx0), my = sqrt(dy0);
         double w = omega;
-        if (mx > 1e-10 && my > 1e-10) w = exp(0.5 * log(my / mx) + 0.5 * log(omega));
+        if (mx > 1e-10 && my > 1e-10 && c.theta > 0.0 && kkt >= c.freeze)
+            w = exp(c.theta * log(my / mx) + (1.0 - c.theta) * log(omega));
         c.omega[b] = w;
         c.tau[b] = c.eta[b] / w;
         c.sigma[b] = c.eta[b] * w;
@@ -781,17 +784,26 @@ private:
         c.tol = o_.relative_tolerance;
         c.limit = o_.iteration_limit;
         c.count = B_;
+        const PrimalWeightRule pw = primal_weight_rule();
+        c.theta = pw.theta;
+        c.freeze = pw.freeze;
+        c.beta_suff = pw.beta_suff;
+        c.beta_nec = pw.beta_nec;
+        c.beta_art = pw.beta_art;
         return c;
     }
 
     void reset_control() {
         const size_t Bs = B_;
         std::vector<double> tau(Bs), sigma(Bs), neg(Bs, -1.0), inf(Bs, std::numeric_limits<double>::infinity());
+        std::vector<double> w(Bs);
+        const double start = primal_weight_rule().start;
         for (int b = 0; b < B_; ++b) {
-            tau[b] = h_eta_[b] / h_omega0_[b];
-            sigma[b] = h_eta_[b] * h_omega0_[b];
+            w[b] = h_omega0_[b] * start;
+            tau[b] = h_eta_[b] / w[b];
+            sigma[b] = h_eta_[b] * w[b];
         }
-        VK_CUDA(cudaMemcpyAsync(omega_.get(), h_omega0_.data(), Bs * 8, cudaMemcpyHostToDevice, s_));
+        VK_CUDA(cudaMemcpyAsync(omega_.get(), w.data(), Bs * 8, cudaMemcpyHostToDevice, s_));
         VK_CUDA(cudaMemcpyAsync(tau_.get(), tau.data(), Bs * 8, cudaMemcpyHostToDevice, s_));
         VK_CUDA(cudaMemcpyAsync(sigma_.get(), sigma.data(), Bs * 8, cudaMemcpyHostToDevice, s_));
         VK_CUDA(cudaMemcpyAsync(rr_.get(), neg.data(), Bs * 8, cudaMemcpyHostToDevice, s_));
@@ -1846,6 +1858,12 @@ private:
         c.tol = o_.relative_tolerance;
         c.limit = o_.iteration_limit;
         c.count = B_;
+        const PrimalWeightRule pw = primal_weight_rule();
+        c.theta = pw.theta;
+        c.freeze = pw.freeze;
+        c.beta_suff = pw.beta_suff;
+        c.beta_nec = pw.beta_nec;
+        c.beta_art = pw.beta_art;
         return c;
     }
 
@@ -1856,7 +1874,7 @@ private:
     }
 
     void reset_control(const std::vector<int> &invalid) {
-        const double eta = base_.h_eta_[0], w0 = base_.h_omega0_[0];
+        const double eta = base_.h_eta_[0], w0 = base_.h_omega0_[0] * primal_weight_rule().start;
         fill(eta_, eta);
         fill(omega_, w0);
         fill(tau_, eta / w0);
@@ -2080,6 +2098,8 @@ void for_members(int count, F &&f) {
     std::atomic<int> next{0};
     std::vector<std::exception_ptr> err(count);
     auto work = [&] {
+        const bool was = serial_host_work();
+        set_serial_host_work(true); // no threads of their own inside the members' work
         for (int b = next++; b < count; b = next++) {
             try {
                 f(b);
@@ -2087,9 +2107,14 @@ void for_members(int count, F &&f) {
                 err[b] = std::current_exception();
             }
         }
+        set_serial_host_work(was);
     };
     std::vector<std::thread> pool;
-    for (int t = 1; t < T; ++t) pool.emplace_back(work);
+    try {
+        for (int t = 1; t < T; ++t) pool.emplace_back(work);
+    } catch (const std::system_error &) {
+        // fewer threads than asked for: the ones running (and this one) share the members
+    }
     work();
     for (std::thread &th : pool) th.join();
     for (const std::exception_ptr &e : err)
@@ -2100,29 +2125,20 @@ double active_tolerance(const vk_options &o) { return std::max(10.0 * o.primal_t
 
 } // namespace
 
-void batch_solve(const vk_problem *probs, int count, const vk_options &o, vk_result *results) {
+namespace {
+
+// Checks of an independent batch (every member with vk_pdhg_create's rules,
+// over host threads; the first failing member in order is reported).
+void validate_batch(const vk_problem *probs, int count, const vk_options &o) {
     if (count <= 0) throw InvalidInput("count must be positive");
     if (o.algorithm != VK_ALGO_HALPERN) throw Unsupported("batched solves use VK_ALGO_HALPERN");
-    // every instance checked (over host threads for large batches); the
-    // first failing instance in order is reported, as a sequential scan would
     std::vector<std::string> msgs(count);
     std::vector<char> unsup(count, 0);
-    {
-        std::atomic<int> next{0};
-        auto work = [&] {
-            for (int b = next++; b < count; b = next++) {
-                bool unsupported = false;
-                msgs[b] = validate_problem(probs[b], o, unsupported);
-                unsup[b] = unsupported ? 1 : 0;
-            }
-        };
-        const unsigned hw = std::thread::hardware_concurrency();
-        const int T = count < 8 ? 1 : std::min<int>({count, 16, static_cast<int>(hw == 0 ? 1 : hw)});
-        std::vector<std::thread> pool;
-        for (int t = 1; t < T; ++t) pool.emplace_back(work);
-        work();
-        for (std::thread &th : pool) th.join();
-    }
+    for_members(count, [&](int b) {
+        bool unsupported = false;
+        msgs[b] = validate_problem(probs[b], o, unsupported);
+        unsup[b] = unsupported ? 1 : 0;
+    });
     int64_t m = 0, n = 0, nnz = 0;
     for (int b = 0; b < count; ++b) {
         if (!msgs[b].empty()) {
@@ -2138,29 +2154,10 @@ void batch_solve(const vk_problem *probs, int count, const vk_options &o, vk_res
     }
     if (m >= (int64_t(1) << 31) || n >= (int64_t(1) << 31) || nnz >= (int64_t(1) << 31))
         throw Unsupported("the batch exceeds the int32 index range of the device structures");
-    const auto t0 = std::chrono::steady_clock::now();
-    {
-        BatchEngine eng(probs, count, o);
-        eng.solve(results);
-    }
-    // split duals and the reference's residuals of every member whose caller
-    // asked for dual arrays (and passed x, y)
-    for_members(count, [&](int b) {
-        vk_result &r = results[b];
-        if (!wants_duals(r) || !r.x || (!r.y && probs[b].A.rows > 0)) return;
-        const vk_problem &p = probs[b];
-        std::vector<double> s;
-        postprocess_member(p.A, p.c, p.row_lower, p.row_upper, p.var_lower, p.var_upper, active_tolerance(o), r, s);
-    });
-    if (o.verbose > 0)
-        std::fprintf(stderr, "[vikalp_b200] batch: total incl. release       %8.3f s\n", seconds_since(t0));
 }
 
-
-// Validates the model (LP only) and solves `count` relaxations of it that
-// differ in variable bounds / warm start.
-void batch_solve_shared(const vk_problem &p, int count, const double *lower, const double *upper,
-                        const double *warm, const vk_options &o, vk_result *results) {
+// Checks of a node batch (the model, LP only, and the batch's size).
+void validate_shared(const vk_problem &p, int count, const vk_options &o) {
     if (count <= 0) throw InvalidInput("count must be positive");
     if (o.algorithm != VK_ALGO_HALPERN) throw Unsupported("batched solves use VK_ALGO_HALPERN");
     bool unsupported = false;
@@ -2169,20 +2166,27 @@ void batch_solve_shared(const vk_problem &p, int count, const double *lower, con
         if (unsupported) throw Unsupported(msg);
         throw InvalidInput(msg);
     }
-    if (p.Q.rows > 0 && p.Q.row_offsets && p.Q.row_offsets[p.Q.rows] > 0)
-        throw Unsupported("batched solves take LPs");
+    if (p.Q.rows > 0 && p.Q.row_offsets && p.Q.row_offsets[p.Q.rows] > 0) throw Unsupported("batched solves take LPs");
     const int64_t ld = (static_cast<int64_t>(count) + 127) / 128 * 128;
     if ((p.A.cols + 1) * ld >= (int64_t(1) << 40) || count >= (1 << 24))
         throw Unsupported("the batch is too large for one device");
-    const auto t0 = std::chrono::steady_clock::now();
-    std::chrono::steady_clock::time_point t1;
-    {
-        SharedEngine eng(p, count, o);
-        eng.solve(lower, upper, warm, results);
-        t1 = std::chrono::steady_clock::now();
-    }
-    // split duals and the reference's residuals of every node whose caller
-    // asked for dual arrays (and passed x, y), under the node's own bounds
+}
+
+// Split duals and the reference's residuals of every independent member whose
+// caller asked for dual arrays (and passed x, y).
+void post_batch(const vk_problem *probs, int count, const vk_options &o, vk_result *results) {
+    for_members(count, [&](int b) {
+        vk_result &r = results[b];
+        if (!wants_duals(r) || !r.x || (!r.y && probs[b].A.rows > 0)) return;
+        const vk_problem &p = probs[b];
+        std::vector<double> s;
+        postprocess_member(p.A, p.c, p.row_lower, p.row_upper, p.var_lower, p.var_upper, active_tolerance(o), r, s);
+    });
+}
+
+// The same for every node, under the node's own bounds.
+void post_shared(const vk_problem &p, int count, const double *lower, const double *upper, const vk_options &o,
+                 vk_result *results) {
     const int64_t n = p.A.cols;
     for_members(count, [&](int b) {
         vk_result &r = results[b];
@@ -2192,10 +2196,78 @@ void batch_solve_shared(const vk_problem &p, int count, const double *lower, con
         std::vector<double> s;
         postprocess_member(p.A, p.c, p.row_lower, p.row_upper, lo, hi, active_tolerance(o), r, s);
     });
+}
+
+} // namespace
+
+void batch_solve(const vk_problem *probs, int count, const vk_options &o, vk_result *results) {
+    validate_batch(probs, count, o);
+    const auto t0 = std::chrono::steady_clock::now();
+    {
+        BatchEngine eng(probs, count, o);
+        eng.solve(results);
+    }
+    post_batch(probs, count, o, results);
+    if (o.verbose > 0)
+        std::fprintf(stderr, "[vikalp_b200] batch: total incl. release       %8.3f s\n", seconds_since(t0));
+}
+
+// Validates the model (LP only) and solves `count` relaxations of it that
+// differ in variable bounds / warm start.
+void batch_solve_shared(const vk_problem &p, int count, const double *lower, const double *upper,
+                        const double *warm, const vk_options &o, vk_result *results) {
+    validate_shared(p, count, o);
+    const auto t0 = std::chrono::steady_clock::now();
+    std::chrono::steady_clock::time_point t1;
+    {
+        SharedEngine eng(p, count, o);
+        eng.solve(lower, upper, warm, results);
+        t1 = std::chrono::steady_clock::now();
+    }
+    post_shared(p, count, lower, upper, o, results);
     if (o.verbose > 0) {
         std::fprintf(stderr, "[vikalp_b200] shared: release (graphs, memory)  %8.3f s\n", seconds_since(t1));
         std::fprintf(stderr, "[vikalp_b200] shared: total incl. release      %8.3f s\n", seconds_since(t0));
     }
+}
+
+void batch_solve_together(const vk_problem &shared, int node_count, const double *lower, const double *upper,
+                          const double *warm, const vk_problem *probs, int count, const vk_options &o,
+                          vk_result *node_results, vk_result *results) {
+    validate_shared(shared, node_count, o);
+    validate_batch(probs, count, o);
+    const auto t0 = std::chrono::steady_clock::now();
+    {
+        // both set-ups first (they allocate and free device memory, which
+        // synchronises the device), then both iteration loops at once, each
+        // engine on its own stream from its own host thread
+        SharedEngine nodes(shared, node_count, o);
+        BatchEngine lps(probs, count, o);
+        if (o.verbose > 0)
+            std::fprintf(stderr, "[vikalp_b200] together: both set-ups         %8.3f s\n", seconds_since(t0));
+        std::exception_ptr err;
+        std::thread other([&] {
+            try {
+                VK_CUDA(cudaSetDevice(o.device));
+                lps.solve(results);
+            } catch (...) {
+                err = std::current_exception();
+            }
+        });
+        std::exception_ptr mine;
+        try {
+            nodes.solve(lower, upper, warm, node_results);
+        } catch (...) {
+            mine = std::current_exception();
+        }
+        other.join();
+        if (mine) std::rethrow_exception(mine);
+        if (err) std::rethrow_exception(err);
+    }
+    post_shared(shared, node_count, lower, upper, o, node_results);
+    post_batch(probs, count, o, results);
+    if (o.verbose > 0)
+        std::fprintf(stderr, "[vikalp_b200] together: total incl. release   %8.3f s\n", seconds_since(t0));
 }
 
 } // namespace vk

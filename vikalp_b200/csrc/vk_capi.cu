@@ -499,6 +499,25 @@ int vk_batch_solve_shared(const vk_problem *problem, int32_t count, const double
     });
 }
 
+int vk_batch_solve_together(const vk_problem *problem, int32_t node_count, const double *lower,
+                            const double *upper, const double *warm, const vk_problem *problems, int32_t count,
+                            const vk_options *opts, vk_result *node_results, vk_result *results) {
+    return guarded([&] {
+        if (!problem || !problems || !node_results || !results || node_count <= 0 || count <= 0)
+            return set_error(VK_ERR_INVALID, "invalid argument");
+        vk_options o;
+        if (opts)
+            o = *opts;
+        else {
+            vk_default_options(&o);
+            o.algorithm = VK_ALGO_HALPERN;
+        }
+        vk::batch_solve_together(*problem, node_count, lower, upper, warm, problems, count, o, node_results,
+                                 results);
+        return VK_OK;
+    });
+}
+
 void vk_default_adjoint_options(vk_adjoint_options *o) {
     if (!o) return;
     o->active_tolerance = 1e-6;

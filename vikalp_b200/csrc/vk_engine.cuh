@@ -4,8 +4,45 @@
 #include "vk_solver.h"
 
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 
 namespace vk {
+
+// Primal weight and restart rule of the restarted Halpern scheme, the same for
+// the single-instance engine and every member of a batch. The primal weight
+// omega starts at `start` x omega_0 (omega_0 = |c^| / |b^|, scaled) and at
+// every restart moves to exp(theta log(|dy|/|dx|) + (1 - theta) log omega),
+// |dx|, |dy| the moves since the last restart point (theta = 0: fixed), as
+// long as the relative KKT error is at least `freeze` (below it, omega keeps
+// its value).
+// Restart when the fixed-point residual r fell below beta_suff x its value at
+// the last restart, or below beta_nec x and grew since the previous check, or
+// when the iterations since the restart reach beta_art x all iterations.
+// VIKALP_B200_PRIMAL_WEIGHT="start,theta,freeze" and
+// VIKALP_B200_RESTART="sufficient,necessary,artificial" override the
+// defaults (experiments; every engine reads them at the start of a solve).
+struct PrimalWeightRule {
+    double start = 1.0, theta = 0.5, freeze = 0.0;
+    double beta_suff = 0.2, beta_nec = 0.8, beta_art = 0.36;
+};
+
+inline PrimalWeightRule primal_weight_rule() {
+    PrimalWeightRule r;
+    if (const char *e = std::getenv("VIKALP_B200_PRIMAL_WEIGHT"); e && *e) {
+        double a = r.start, b = r.theta, f = r.freeze;
+        const int got = std::sscanf(e, "%lf,%lf,%lf", &a, &b, &f);
+        if (got >= 1 && a > 0.0) r.start = a;
+        if (got >= 2 && b >= 0.0 && b <= 1.0) r.theta = b;
+        if (got >= 3 && f >= 0.0) r.freeze = f;
+    }
+    if (const char *e = std::getenv("VIKALP_B200_RESTART"); e && *e) {
+        double a = r.beta_suff, b = r.beta_nec, c = r.beta_art;
+        if (std::sscanf(e, "%lf,%lf,%lf", &a, &b, &c) == 3 && a > 0.0 && a < 1.0 && b > 0.0 && b < 1.0 && c > 0.0)
+            r.beta_suff = a, r.beta_nec = b, r.beta_art = c;
+    }
+    return r;
+}
 
 struct RunInfo {
     int status = VK_STATUS_NOT_SOLVED;

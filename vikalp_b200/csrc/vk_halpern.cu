@@ -39,7 +39,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
-#include <cstdlib>
 #include <limits>
 
 namespace vk {
@@ -59,7 +58,7 @@ struct HalCtl {
     double rel_p, rel_d, rel_gap, kkt;
     double bnorm, cnorm, offset, tol;
     double knorm, lq, rho, pad_d; // sigma_max(K), lambda_max(Q^) (0: LP), reflection
-    double theta, omega_lo, omega_hi;       // primal-weight smoothing and clamp
+    double theta, freeze;                   // primal-weight smoothing; no update below this KKT
     double beta_suff, beta_nec, beta_art;   // restart thresholds
     long long k_base, total, limit, restarts, checks;
     int done, status, restart_now, pad;
@@ -72,35 +71,6 @@ struct HalCtl {
 // rho = 0.99 (1 - 1/(2 kappa)), kappa = (1/tau - sigma |K|^2) / L, which keeps
 // (1+rho) T - rho I nonexpansive (Condat's bound on the relaxation of the
 // primal-dual iteration with a smooth term).
-// Primal weight and restart rule of the Halpern scheme. Defaults: omega
-// starts at omega_0 = |c^| / |b^|, moves at each restart to the smoothed
-// log-ratio of the restart points' moves (theta = 0.5), unclamped; restart
-// thresholds 0.2 / 0.8 / 0.36. VIKALP_B200_PRIMAL_WEIGHT="start,theta,lo,hi"
-// (start, lo, hi as multiples of omega_0) and
-// VIKALP_B200_RESTART="sufficient,necessary,artificial" override them.
-struct PrimalWeightRule {
-    double start = 1.0, theta = 0.5, lo = 0.0, hi = std::numeric_limits<double>::infinity();
-    double beta_suff = 0.2, beta_nec = 0.8, beta_art = 0.36;
-};
-
-inline PrimalWeightRule primal_weight_rule() {
-    PrimalWeightRule r;
-    if (const char *e = std::getenv("VIKALP_B200_PRIMAL_WEIGHT"); e && *e) {
-        double a = r.start, b = r.theta, c = r.lo, d = r.hi;
-        const int got = std::sscanf(e, "%lf,%lf,%lf,%lf", &a, &b, &c, &d);
-        if (got >= 1 && a > 0.0) r.start = a;
-        if (got >= 2 && b >= 0.0 && b <= 1.0) r.theta = b;
-        if (got >= 3 && c >= 0.0) r.lo = c;
-        if (got >= 4 && d > 0.0) r.hi = d;
-    }
-    if (const char *e = std::getenv("VIKALP_B200_RESTART"); e && *e) {
-        double a = r.beta_suff, b = r.beta_nec, c = r.beta_art;
-        if (std::sscanf(e, "%lf,%lf,%lf", &a, &b, &c) == 3 && a > 0.0 && a < 1.0 && b > 0.0 && b < 1.0 && c > 0.0)
-            r.beta_suff = a, r.beta_nec = b, r.beta_art = c;
-    }
-    return r;
-}
-
 __host__ __device__ inline void step_params(double knorm, double lq, double omega, double &eta, double &rho) {
     if (!(lq > 0.0)) {
         eta = knorm > 0.0 ? 0.99 / knorm : 1.0;
@@ -436,8 +406,8 @@ __global__ void __launch_bounds__(kControlThreads)
         c.r_prev = r;
         if (restart) {
             const double mx = sqrt(dx0), my = sqrt(dy0);
-            if (mx > 1e-10 && my > 1e-10 && c.theta > 0.0)
-                c.omega = fmin(c.omega_hi, fmax(c.omega_lo, exp(c.theta * log(my / mx) + (1.0 - c.theta) * log(c.omega))));
+            if (mx > 1e-10 && my > 1e-10 && c.theta > 0.0 && c.kkt >= c.freeze)
+                c.omega = exp(c.theta * log(my / mx) + (1.0 - c.theta) * log(c.omega));
             step_params(c.knorm, c.lq, c.omega, c.eta, c.rho);
             c.tau = c.eta / c.omega;
             c.sigma = c.eta * c.omega;
@@ -450,6 +420,35 @@ __global__ void __launch_bounds__(kControlThreads)
         }
     }
     *ctl = c;
+}
+
+struct KktEval {
+    double rel_p, rel_d, rel_gap, kkt;
+};
+
+// The relative KKT error of the KKT passes' partial sums (the evaluation part
+// of check_control_kernel, without any decision). One block.
+__global__ void __launch_bounds__(kControlThreads)
+    kkt_eval_kernel(const HalCtl *ctl, const double *pkr, const double *pkc, int grid_row, int grid_col,
+                    KktEval *out) {
+    __shared__ double scratch[32];
+    double s[kKktRowSums + kKktColSums];
+    int o = 0;
+    for (int r = 0; r < kKktRowSums; ++r) s[o++] = block_reduce_range(pkr, grid_row, kKktRowSums, r, scratch);
+    for (int r = 0; r < kKktColSums; ++r) s[o++] = block_reduce_range(pkc, grid_col, kKktColSums, r, scratch);
+    if (threadIdx.x != 0) return;
+    const HalCtl &c = *ctl;
+    const double rp2 = s[0], dobj_r = s[1], viol2 = s[2];
+    const double rd2 = s[3], dobj_c = s[4], box2 = s[6], quad = s[7];
+    const double pobj = s[5] + 0.5 * quad + c.offset;
+    const double dobj = dobj_r + dobj_c - 0.5 * quad + c.offset;
+    KktEval e;
+    e.rel_p = (sqrt(rp2) + sqrt(box2)) / (1.0 + c.bnorm);
+    e.rel_d = sqrt(rd2 + viol2) / (1.0 + c.cnorm);
+    e.rel_gap = fabs(pobj - dobj) / (1.0 + fabs(pobj) + fabs(dobj));
+    e.kkt = smax(smax(e.rel_p, e.rel_d), e.rel_gap);
+    if (!(e.kkt == e.kkt)) e.kkt = std::numeric_limits<double>::infinity();
+    *out = e;
 }
 
 template <class T>
@@ -518,6 +517,8 @@ public:
         step_size();
         log.mark("step size (power iteration)");
         ctl_.reset(1);
+        evalctl_.reset(1);
+        evalout_.reset(1);
         hctl_.reset(1);
         pc_.reset(static_cast<size_t>(kMaxGrid) * kColCheckSums);
         pr_.reset(static_cast<size_t>(kMaxGrid) * kRowCheckSums);
@@ -564,8 +565,7 @@ public:
         const PrimalWeightRule pw = primal_weight_rule();
         c.omega = omega0_ * pw.start;
         c.theta = pw.theta;
-        c.omega_lo = omega0_ * pw.lo;
-        c.omega_hi = omega0_ * pw.hi;
+        c.freeze = pw.freeze;
         c.beta_suff = pw.beta_suff;
         c.beta_nec = pw.beta_nec;
         c.beta_art = pw.beta_art;
@@ -633,43 +633,73 @@ public:
         launches_ = 0;
         bool timed_out = false;
         long long fp32_iters = 0;
+        bool confirmed = false; // mixed: the float32 answer passed the float64 evaluation
         if (mixed_) {
             copy_state<float, double>(s64_, s32_);
             if (!g32_) g32_ = capture(s32_);
-            // float32 phase: stop on the tolerance, on the limit, or when the
-            // float32 KKT error stops improving
+            // float32 phase. When its own (float32) KKT evaluation reaches the
+            // tolerance, the point is evaluated again in float64 with no
+            // float64 iteration: accepted there, the solve ends; otherwise the
+            // float32 target is halved (down to kFp32Floor, about the noise of
+            // a float32 evaluation) and the float32 iterations go on. The
+            // phase also ends on the limit, or on a plateau: no halving of the
+            // best float32 KKT error over the last max(32 checks, a quarter
+            // of the checks so far) once it is below 1e-3.
+            constexpr double kFp32Floor = 1e-7;
             double best = std::numeric_limits<double>::infinity();
-            int stall = 0;
-            const double fp32_floor = 1e-7;
+            long long best_at = 0;
+            double target = o_.relative_tolerance;
             for (;;) {
                 if (over_time(started)) {
                     timed_out = true;
                     break;
                 }
                 poll_chunk(g32_);
-                const HalCtl &h = hctl_[0];
-                if (h.done) break;
-                if (h.kkt < 0.7 * best) {
+                HalCtl h = hctl_[0];
+                if (h.done) {
+                    if (h.status != VK_STATUS_OPTIMAL) break;
+                    const double k64 = evaluate64();
+                    if (k64 <= o_.relative_tolerance) {
+                        confirmed = true;
+                        break;
+                    }
+                    if (target * 0.5 < kFp32Floor) break;
+                    target *= 0.5;
+                    h.done = 0;
+                    h.status = VK_STATUS_NOT_SOLVED;
+                    h.tol = target;
+                    VK_CUDA(cudaMemcpyAsync(ctl_.get(), &h, sizeof(h), cudaMemcpyHostToDevice, s_));
+                    continue;
+                }
+                if (h.kkt < 0.5 * best) {
                     best = h.kkt;
-                    stall = 0;
-                } else if (++stall >= 6 && h.kkt < 1e-3) {
+                    best_at = h.checks;
+                } else if (h.kkt < 1e-3 && h.checks - best_at >= std::max<long long>(32, h.checks / 4)) {
                     break;
                 }
-                if (h.kkt < smax(fp32_floor, 0.5 * o_.relative_tolerance)) break;
             }
             fp32_iters = hctl_[0].total;
             // hand the float32 state to float64 and re-open the control block
             copy_state<double, float>(s32_, s64_);
             HalCtl h = hctl_[0];
-            if (h.status == VK_STATUS_OPTIMAL || h.status == VK_STATUS_NOT_SOLVED ||
-                h.status == VK_STATUS_ITERATION_LIMIT) {
+            if (confirmed) {
+                h.done = 1;
+                h.status = VK_STATUS_OPTIMAL;
+                h.kkt = k64_.kkt;
+                h.rel_p = k64_.rel_p;
+                h.rel_d = k64_.rel_d;
+                h.rel_gap = k64_.rel_gap;
+                VK_CUDA(cudaMemcpyAsync(ctl_.get(), &h, sizeof(h), cudaMemcpyHostToDevice, s_));
+            } else if (h.status == VK_STATUS_OPTIMAL || h.status == VK_STATUS_NOT_SOLVED ||
+                       h.status == VK_STATUS_ITERATION_LIMIT) {
                 h.done = 0;
                 h.status = VK_STATUS_NOT_SOLVED;
+                h.tol = o_.relative_tolerance;
                 h.limit = o_.iteration_limit + std::max<long long>(chunk_, 0); // the polish gets at least one check
                 VK_CUDA(cudaMemcpyAsync(ctl_.get(), &h, sizeof(h), cudaMemcpyHostToDevice, s_));
             }
         }
-        if (!timed_out) {
+        if (!timed_out && !confirmed) {
             if (!g64_) g64_ = capture(s64_);
             for (;;) {
                 if (over_time(started)) {
@@ -708,6 +738,28 @@ public:
     void set_limits(const vk_options &o) override { o_ = o; }
 
 private:
+    // Relative KKT error, in float64, of the float32 state's last (x^, y^):
+    // converted to float64, then the two float64 KKT passes and one
+    // evaluation kernel -- no iteration. Leaves the float64 x^, y^ in place.
+    double evaluate64() {
+        const int m = dm_.m, n = dm_.n;
+        convert_kernel<double, float><<<grid1d(n), 256, 0, s_>>>(s32_.xhat.get(), n, s64_.xhat.get());
+        if (m > 0) convert_kernel<double, float><<<grid1d(m), 256, 0, s_>>>(s32_.yhat.get(), m, s64_.yhat.get());
+        VK_LAUNCH_CHECK();
+        HalCtl e = hctl_[0]; // its norms and offset; done = 0 so the passes run
+        e.done = 0;
+        VK_CUDA(cudaMemcpyAsync(evalctl_.get(), &e, sizeof(e), cudaMemcpyHostToDevice, s_));
+        int grid_col = 0;
+        const int grid_row = kkt_passes(s64_, grid_col, evalctl_.get());
+        kkt_eval_kernel<<<1, kControlThreads, 0, s_>>>(evalctl_.get(), pkr_.get(), pkc_.get(), grid_row, grid_col,
+                                                      evalout_.get());
+        VK_LAUNCH_CHECK();
+        VK_CUDA(cudaMemcpyAsync(&k64_, evalout_.get(), sizeof(KktEval), cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaStreamSynchronize(s_));
+        check_device_error(s_);
+        return k64_.kkt;
+    }
+
     bool over_time(std::chrono::steady_clock::time_point t0) const {
         return std::isfinite(o_.time_limit_seconds) && seconds_since(t0) >= o_.time_limit_seconds;
     }
@@ -938,10 +990,10 @@ private:
 
     // QP: qx = Q^ v (no-op for an LP, and skipped once the solve is done).
     template <class T>
-    void q_pass(HalState<T> &st, const T *v) {
+    void q_pass(HalState<T> &st, const T *v, const HalCtl *ctl = nullptr) {
         if (!dm_.qp) return;
         QStore<T> e;
-        e.ctl = ctl_.get();
+        e.ctl = ctl ? ctl : ctl_.get();
         e.y = st.qx.get();
         launch_tiles<T, T, 1, false>(view(dm_.q, st.q.get()), Gathers<T, 1>{{v}}, e, s_);
     }
@@ -990,11 +1042,12 @@ private:
     }
 
     template <class T>
-    int kkt_passes(HalState<T> &st, int &grid_col) {
+    int kkt_passes(HalState<T> &st, int &grid_col, const HalCtl *ctl = nullptr) {
+        if (!ctl) ctl = ctl_.get();
         int gr = 0;
         if (st.m > 0) {
             KktRowEpi<T> r;
-            r.ctl = ctl_.get();
+            r.ctl = ctl;
             r.yhat = st.yhat.get();
             r.rl = st.rl.get();
             r.ru = st.ru.get();
@@ -1002,9 +1055,9 @@ private:
             r.partials = pkr_.get();
             gr = launch_tiles<T, T, 1, false>(view(dm_.a, st.ka.get()), Gathers<T, 1>{{st.xhat.get()}}, r, s_);
         }
-        q_pass(st, st.xhat.get());
+        q_pass(st, st.xhat.get(), ctl);
         KktColEpi<T> c;
-        c.ctl = ctl_.get();
+        c.ctl = ctl;
         c.qx = dm_.qp ? st.qx.get() : nullptr;
         c.xhat = st.xhat.get();
         c.c = st.c.get();
@@ -1025,8 +1078,10 @@ private:
     DevBuf<double> rs_, cs_;
     HalState<double> s64_;
     HalState<float> s32_;
-    DevBuf<HalCtl> ctl_;
+    DevBuf<HalCtl> ctl_, evalctl_;
     HostBuf<HalCtl> hctl_;
+    DevBuf<KktEval> evalout_;
+    KktEval k64_{};
     DevBuf<double> pc_, pr_, pkr_, pkc_;
     double knorm_ = 0.0, lq_ = 0.0, omega0_ = 1.0, bnorm_ = 0.0, cnorm_ = 0.0;
     cudaGraphExec_t g64_ = nullptr, g32_ = nullptr;

@@ -7,10 +7,18 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <system_error>
 #include <thread>
 #include <vector>
 
 namespace vk {
+
+namespace {
+thread_local bool t_serial_host_work = false;
+} // namespace
+
+bool serial_host_work() { return t_serial_host_work; }
+void set_serial_host_work(bool on) { t_serial_host_work = on; }
 
 // ---------------------------------------------------------------------------
 // Validation: Model::validate (Model.cpp:118-199) restricted to what a
@@ -28,7 +36,9 @@ template <class F>
 int64_t first_failure(int64_t count, int64_t work, F check, int &code) {
     constexpr int64_t kSerial = int64_t(1) << 20;
     const unsigned hw = std::thread::hardware_concurrency();
-    const int T = work < kSerial || count < 2 ? 1 : static_cast<int>(std::min<unsigned>(hw == 0 ? 1 : hw, 16));
+    const int T = work < kSerial || count < 2 || serial_host_work()
+                      ? 1
+                      : static_cast<int>(std::min<unsigned>(hw == 0 ? 1 : hw, 16));
     if (T <= 1) return check(0, count, code);
     std::vector<int64_t> at(T, -1);
     std::vector<int> codes(T, 0);
@@ -38,7 +48,13 @@ int64_t first_failure(int64_t count, int64_t work, F check, int &code) {
         const int64_t b = count * t / T, e = count * (t + 1) / T;
         at[t] = check(b, e, codes[t]);
     };
-    for (int t = 1; t < T; ++t) pool.emplace_back(part, t);
+    int started = 1;
+    try {
+        for (; started < T; ++started) pool.emplace_back(part, started);
+    } catch (const std::system_error &) {
+        // no more threads to be had: the parts not started run here
+    }
+    for (int t = started; t < T; ++t) part(t);
     part(0);
     for (auto &th : pool) th.join();
     for (int t = 0; t < T; ++t)

@@ -36,6 +36,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <limits>
+#include <string>
 #include <vector>
 
 namespace vk {
@@ -438,9 +439,13 @@ public:
         check_device_error(s_);
         pp = PassProfile{};
         pp.count = kinds;
-        pp.name[0] = "column pass (K'y, primal step)";
-        pp.name[1] = "control + primal kernel";
-        pp.name[2] = dm_.qp ? "Q pass + row pass" : "row pass (K x, dual step)";
+        // names carry the kernel variant each pass ran (the tuner's pick)
+        const auto tag = [&](int v) { return exact_ ? std::string(", sequential") : ", variant " + std::to_string(v); };
+        prof_names_[0] = "column pass (K'y, primal step)" + tag(col_view().variant);
+        prof_names_[1] = "control + primal kernel";
+        prof_names_[2] = (dm_.qp ? std::string("Q pass + row pass") : std::string("row pass (K x, dual step)")) +
+                         tag(row_view().variant);
+        for (int q = 0; q < kinds; ++q) pp.name[q] = prof_names_[q].c_str();
         const double s = 8.0; // float64 values and vectors
         const double nnz = static_cast<double>(dm_.nnz);
         // Algorithmic bytes: values + int32 indices, int32 offsets, the
@@ -725,6 +730,7 @@ private:
         cudaGraphDestroy(g);
     }
 
+    std::string prof_names_[3]; // pass names handed out by profile()
     const DeviceModel &dm_;
     vk_options o_;
     cudaStream_t s_;

@@ -69,6 +69,12 @@ double *dvec_ptr(vk_dvec *v);
 const double *dvec_ptr(const vk_dvec *v);
 int64_t dvec_size(const vk_dvec *v);
 
+// Host work already spread over threads (a batch's members) sets this on its
+// workers, so the scans inside (validate_problem) stay on their thread
+// instead of starting threads of their own.
+bool serial_host_work();
+void set_serial_host_work(bool on);
+
 // Validation of a vk_problem with the reference's rules and messages.
 // Returns "" when valid. `unsupported` is set when the failure maps to
 // SolveStatus::UnsupportedModel instead of InvalidModel.
@@ -85,6 +91,11 @@ void batch_solve(const vk_problem *problems, int count, const vk_options &o, vk_
 // Relaxations of one LP differing in variable bounds / warm start (vk_batch.cu).
 void batch_solve_shared(const vk_problem &p, int count, const double *lower, const double *upper,
                         const double *warm, const vk_options &o, vk_result *results);
+// A node batch and an independent batch with both device loops in flight at
+// once (vk_batch.cu).
+void batch_solve_together(const vk_problem &shared, int node_count, const double *lower, const double *upper,
+                          const double *warm, const vk_problem *probs, int count, const vk_options &o,
+                          vk_result *node_results, vk_result *results);
 // Active-set adjoint of solved LPs (vk_adjoint.cu).
 void lp_adjoint(const vk_problem *probs, int count, const double *x, const double *y, const double *g, double w_obj,
                 const vk_adjoint_options &o, double *dc, double *db, double *da, vk_adjoint_info *info);
