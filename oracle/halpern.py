@@ -141,9 +141,9 @@ def rel_kkt(inst, x, y, lower=None, upper=None):
 # THETA at each restart, restart thresholds RESTART = (sufficient, necessary,
 # artificial).
 OMEGA_START = 1.0
-THETA = 0.5
+THETA = 0.2
 FREEZE = 0.0  # no primal-weight update once the relative KKT error is below this
-RESTART = (0.2, 0.8, 0.36)
+RESTART = (0.2, 0.8, 0.2)
 
 
 def solve(inst, tol=1e-6, iteration_limit=100000, check_every=64, rho=None, warm=None, lower=None, upper=None,

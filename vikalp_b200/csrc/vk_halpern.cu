@@ -21,9 +21,10 @@
 // applies the restart rule on the fixed-point residual
 //   r = sqrt(omega |x^ - x|^2 + |y^ - y|^2 / omega)
 // (restart when r <= 0.2 r_restart, or r <= 0.8 r_restart and r grew since the
-// previous check, or k >= 0.36 * total iterations), restarting at (x^, y^) and
-// updating the primal weight omega by the smoothed log-ratio of the moves of
-// the restart points. The chunk of check_every iterations is one CUDA graph.
+// previous check, or k >= 0.2 * total iterations; PrimalWeightRule,
+// vk_engine.cuh), restarting at (x^, y^) and updating the primal weight omega
+// by the smoothed (theta = 0.2) log-ratio of the moves of the restart points.
+// The chunk of check_every iterations is one CUDA graph.
 //
 // Setup: 10 Ruiz infinity-norm passes then one Pock-Chambolle (alpha = 1)
 // pass give R and D; eta = 0.99 / sigma_max(K) with sigma_max from power
