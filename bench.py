@@ -396,11 +396,15 @@ def main():
                     help="only run the 512-node shared-matrix batch for this many iterations (for ncu captures)")
     ap.add_argument("--profile-iter", type=int, default=0,
                     help="only run this many reference-scheme iterations on the large LP (for ncu captures)")
+    ap.add_argument("--profile-halpern", choices=["fp64", "mixed"], default=None,
+                    help="only run 256 Halpern-scheme iterations on the large LP (for ncu captures)")
     args = ap.parse_args()
     if args.profile_spmv:
         return profile_spmv(args.profile_spmv, args.transpose)
     if args.profile_iter:
         return profile_iterations(args.profile_iter)
+    if args.profile_halpern:
+        return profile_halpern(args.profile_halpern)
     if args.profile_shared:
         return profile_shared(args.profile_shared)
     K, W = max(1, args.steps), max(3, args.warmup)
@@ -556,6 +560,21 @@ def profile_iterations(iterations):
     inst = synthetic.workload_large_lp()
     with vk.Pdhg(inst, algorithm="reference", check_every=CHUNK) as h:
         r = h.solve(iteration_limit=iterations, primal_tolerance=0.0, dual_tolerance=0.0, duals=False)
+    torch.cuda.synchronize()
+    print(f"ok iterations={r['iterations']} status={r['status']}")
+    return 0
+
+
+def profile_halpern(precision, iterations=256):
+    """`iterations` Halpern-scheme iterations on the large LP (the passes the
+    time-to-tolerance figure runs), for ncu captures."""
+    import torch
+
+    import vikalp_b200 as vk
+    from vikalp_b200 import synthetic
+    inst = synthetic.workload_large_lp()
+    with vk.Pdhg(inst, algorithm="halpern", precision=precision, check_every=CHUNK) as h:
+        r = h.solve(iteration_limit=iterations, relative_tolerance=0.0, duals=False)
     torch.cuda.synchronize()
     print(f"ok iterations={r['iterations']} status={r['status']}")
     return 0

@@ -1072,6 +1072,14 @@ __device__ __forceinline__ void st_vec(T *p, const T (&v)[VEC], const bool (&act
 
 constexpr int kSpmmWarps = 8;
 constexpr int kSpmmMaxR = 4;
+#ifndef VK_SPMM_UNROLL
+#define VK_SPMM_UNROLL 4
+#endif
+#ifndef VK_SPMM_MINB
+#define VK_SPMM_MINB 5
+#endif
+constexpr int kSpmmUnroll = VK_SPMM_UNROLL; // nonzeros of a row in flight per warp step
+constexpr int kSpmmMinBlocks = VK_SPMM_MINB; // resident blocks per SM the registers are held to
 
 // Per-lane instance state common to the epilogues.
 template <class T, int VEC>
@@ -1324,7 +1332,7 @@ struct SpmmMat {
 // slice of X (n * 32 * VEC values) at a time and that slice stays in L2. A
 // group whose instances have all stopped is skipped.
 template <class T, int VEC, class Epi>
-__global__ void __launch_bounds__(kSpmmWarps * 32, 5)
+__global__ void __launch_bounds__(kSpmmWarps * 32, kSpmmMinBlocks)
     spmm_kernel(SpmmMat<T> M, const T *__restrict__ X, int ld, int G, Epi epi, double *__restrict__ partials) {
     constexpr int NR = Epi::NR;
     const int p = blockIdx.x, P = gridDim.x;
@@ -1350,19 +1358,20 @@ __global__ void __launch_bounds__(kSpmmWarps * 32, 5)
             T acc[VEC];
 #pragma unroll
             for (int q = 0; q < VEC; ++q) acc[q] = T(0);
+            constexpr int U = kSpmmUnroll;
             int k = k0;
-            for (; k + 4 <= k1; k += 4) {
-                int cc[4];
-                T vv[4], xv[4][VEC];
+            for (; k + U <= k1; k += U) {
+                int cc[U];
+                T vv[U], xv[U][VEC];
 #pragma unroll
-                for (int t = 0; t < 4; ++t) {
+                for (int t = 0; t < U; ++t) {
                     cc[t] = __ldg(M.ci + k + t);
                     vv[t] = __ldg(M.val + k + t);
                 }
 #pragma unroll
-                for (int t = 0; t < 4; ++t) ldg_vec<T, VEC>(Xb + static_cast<size_t>(cc[t]) * ld, xv[t]);
+                for (int t = 0; t < U; ++t) ldg_vec<T, VEC>(Xb + static_cast<size_t>(cc[t]) * ld, xv[t]);
 #pragma unroll
-                for (int t = 0; t < 4; ++t)
+                for (int t = 0; t < U; ++t)
 #pragma unroll
                     for (int q = 0; q < VEC; ++q) acc[q] += vv[t] * xv[t][q];
             }
@@ -1507,9 +1516,9 @@ public:
         vec32_ = B_ >= 128 ? 4 : 1;
         vec64_ = (B_ >= 64 && ld_ % 64 == 0) ? 2 : 1;
         const int sms = sm_count();
-        // one resident wave of blocks (5 per SM, the launch bound); each walks every instance group
-        P32_ = 5 * sms;
-        P64_ = 5 * sms;
+        // one resident wave of blocks (kSpmmMinBlocks per SM, the launch bound); each walks every instance group
+        P32_ = kSpmmMinBlocks * sms;
+        P64_ = kSpmmMinBlocks * sms;
         control_arrays();
         pmax_ = std::max(P32_, P64_);
         partial_.reset(static_cast<size_t>(pmax_) * kSpmmMaxR * ld_);

@@ -643,12 +643,16 @@ public:
             // float64 iteration: accepted there, the solve ends; otherwise the
             // float32 target is halved (down to kFp32Floor, about the noise of
             // a float32 evaluation) and the float32 iterations go on. The
-            // phase also ends on the limit, or on a plateau: no halving of the
-            // best float32 KKT error over the last max(32 checks, a quarter
-            // of the checks so far) once it is below 1e-3.
+            // phase also ends on the limit, or on a plateau: over a window of
+            // max(32 checks, an eighth of the checks so far) the best float32
+            // KKT error, once below kPlateauFrom, improved by less than
+            // kPlateauGain.
             constexpr double kFp32Floor = 1e-7;
+            constexpr double kPlateauGain = 1.25;
+            constexpr double kPlateauFrom = 1e-3; // early stalls (restart transients) do not count
             double best = std::numeric_limits<double>::infinity();
-            long long best_at = 0;
+            double win_best = best;   // best at the window's start
+            long long win_start = 0;  // check count at the window's start
             double target = o_.relative_tolerance;
             for (;;) {
                 if (over_time(started)) {
@@ -660,6 +664,11 @@ public:
                 if (h.done) {
                     if (h.status != VK_STATUS_OPTIMAL) break;
                     const double k64 = evaluate64();
+                    if (o_.verbose > 0)
+                        std::fprintf(stderr,
+                                     "[vikalp_b200] mixed: float32 KKT %.3e <= target %.3e at %lld iterations; "
+                                     "float64 evaluation %.3e\n",
+                                     h.kkt, target, h.total, k64);
                     if (k64 <= o_.relative_tolerance) {
                         confirmed = true;
                         break;
@@ -672,11 +681,18 @@ public:
                     VK_CUDA(cudaMemcpyAsync(ctl_.get(), &h, sizeof(h), cudaMemcpyHostToDevice, s_));
                     continue;
                 }
-                if (h.kkt < 0.5 * best) {
-                    best = h.kkt;
-                    best_at = h.checks;
-                } else if (h.kkt < 1e-3 && h.checks - best_at >= std::max<long long>(32, h.checks / 4)) {
-                    break;
+                best = std::min(best, h.kkt);
+                if (h.checks - win_start >= std::max<long long>(32, h.checks / 8)) {
+                    if (best < kPlateauFrom && best * kPlateauGain > win_best) {
+                        if (o_.verbose > 0)
+                            std::fprintf(stderr,
+                                         "[vikalp_b200] mixed: float32 plateau at KKT %.3e (best %.3e, %.3e a "
+                                         "window earlier) after %lld iterations; float64 from here\n",
+                                         h.kkt, best, win_best, h.total);
+                        break;
+                    }
+                    win_start = h.checks;
+                    win_best = best;
                 }
             }
             fp32_iters = hctl_[0].total;
