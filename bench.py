@@ -207,12 +207,15 @@ def batched_figures():
         return {"wall_s": round(wall, 3), "status": status, "max_iterations": int(max(r["iterations"] for r in rs)),
                 "max_rel_kkt": float(max(max(r["rel_primal"], r["rel_dual"], r["rel_gap"]) for r in rs))}
 
+    answers = {}
+
     def together(prec):
         t0 = time.perf_counter()
         nodes, lps = vk.batch_solve_together(node_lp, 512, indep, lo, hi, precision=prec, **tol)
         out = summary(nodes + lps, time.perf_counter() - t0)
         out["shared_iterate_s"] = round(nodes[0]["iterate_seconds"], 3)
         out["independent_iterate_s"] = round(lps[0]["iterate_seconds"], 3)
+        answers[prec] = nodes + lps
         return out
 
     def one_after_other(prec):
@@ -228,6 +231,11 @@ def batched_figures():
                        "(m log-uniform 500..20000, n=2m, 8/col; 19.7M nnz), to 1e-6 relative KKT",
            "mixed": together("mixed"), "fp64_batched": together("fp64"),
            "mixed_one_batch_after_the_other": one_after_other("mixed")}
+    # the mixed answers against the float64 ones, instance by instance
+    obj = [abs(a["objective"] - b["objective"]) / (1 + abs(b["objective"]))
+           for a, b in zip(answers["mixed"], answers["fp64"])]
+    out["mixed_vs_fp64"] = {"max_objective_rel_diff": float(max(obj)), "median_objective_rel_diff":
+                            float(statistics.median(obj))}
     # plain float64, every instance one by one
     # (one untimed solve of each kind first, so no one-time cost of the path enters)
     node_t, indep_t, statuses = [], [], {}
