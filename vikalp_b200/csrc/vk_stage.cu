@@ -6,6 +6,7 @@
 #include <cstring>
 #include <exception>
 #include <mutex>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -90,12 +91,12 @@ bool pool_ready() {
 // the pool; after an error it waits for the whole stream s. The first error is
 // rethrown on the calling thread.
 template <class Body>
-void run_staged(int64_t nchunks, cudaStream_t s, Body body) {
+void run_staged(int64_t nchunks, cudaStream_t s, Body body, int max_threads = kStageThreads) {
     int dev = 0;
     VK_CUDA(cudaGetDevice(&dev));
     const unsigned hw = std::thread::hardware_concurrency();
     const int T = static_cast<int>(std::max<int64_t>(
-        1, std::min<int64_t>({static_cast<int64_t>(kStageThreads), nchunks, static_cast<int64_t>(hw == 0 ? 1 : hw)})));
+        1, std::min<int64_t>({static_cast<int64_t>(max_threads), nchunks, static_cast<int64_t>(hw == 0 ? 1 : hw)})));
     std::vector<std::exception_ptr> errs(T);
     auto work = [&](int t) {
         void *buf = nullptr;
@@ -118,8 +119,14 @@ void run_staged(int64_t nchunks, cudaStream_t s, Body body) {
     };
     std::vector<std::thread> pool;
     pool.reserve(T - 1);
-    for (int t = 1; t < T; ++t) pool.emplace_back(work, t);
+    int started = 1;
+    try {
+        for (; started < T; ++started) pool.emplace_back(work, started);
+    } catch (const std::system_error &) {
+        // fewer threads to be had: the calling thread takes the shares not started
+    }
     work(0);
+    for (int t = started; t < T; ++t) work(t);
     for (std::thread &th : pool) th.join();
     for (const std::exception_ptr &e : errs)
         if (e) std::rethrow_exception(e);
@@ -206,7 +213,7 @@ void stage_d2h(void *dst, const void *src, size_t bytes, cudaStream_t s) {
         VK_CUDA(cudaEventSynchronize(ev));
         pending = false;
         std::memcpy(h + off, buf, n);
-    });
+    }, kStageThreadsD2H);
 }
 
 void stage_d2h_many(const StageCopy *copies, int64_t count, cudaStream_t s) {
@@ -232,7 +239,7 @@ void stage_d2h_many(const StageCopy *copies, int64_t count, cudaStream_t s) {
             pending = false;
             std::memcpy(h + off, buf, n);
         }
-    });
+    }, kStageThreadsD2H);
 }
 
 } // namespace vk

@@ -22,6 +22,11 @@ namespace vk {
 constexpr size_t kStageChunk = size_t(4) << 20; // bytes per staged chunk (and per pinned buffer)
 constexpr size_t kStageMin = size_t(16) << 20;  // smaller transfers are not staged
 constexpr int kStageThreads = 4;
+// Device -> host copies write into the caller's memory, which is often fresh
+// (a first touch faults each page in); the kernel serves page faults on
+// different pages in parallel, so downloads spread over more threads. Their
+// extra pinned buffers join the process-wide pool on first use.
+constexpr int kStageThreadsD2H = 16;
 
 // dst (device) <- src (host), `bytes` bytes.
 void stage_h2d(void *dst, const void *src, size_t bytes, cudaStream_t s);
@@ -33,7 +38,7 @@ void stage_h2d_narrow(int *dst, const int64_t *src, int64_t count, cudaStream_t 
 void stage_d2h(void *dst, const void *src, size_t bytes, cudaStream_t s);
 
 // Many device -> host copies (e.g. one result array per batch instance),
-// spread over the staging threads: copy i goes to thread i % T, in pieces of
+// spread over up to kStageThreadsD2H threads: copy i goes to thread i % T, in pieces of
 // at most kStageChunk bytes. Staged when the copies add up to kStageMin bytes.
 struct StageCopy {
     void *dst;
