@@ -127,3 +127,17 @@ def test_qp_solves_to_relative_kkt(qp_small, oracle, precision):
     assert max(k["rel_primal"], k["rel_dual"], k["rel_gap"]) <= KKT_TOL, k
     # objective of the restatement run to 1e-8 relative KKT (48.0767314906966)
     assert abs(r["objective"] - 48.0767314906966) <= 1e-5 * 49.0
+
+
+def test_mixed_float32_answer_confirmed_in_float64(oracle):
+    # the float32 phase reaches the tolerance by its own evaluation; the same
+    # point, evaluated again in float64 (no float64 iteration), is accepted:
+    # every iteration ran in float32 and the answer certifies at 1e-6
+    inst = synthetic.workload_small_lp()
+    r = vk.solve(inst, algorithm="halpern", precision="mixed", iteration_limit=200000, relative_tolerance=1e-6)
+    assert r["status"] == "Optimal", r["message"]
+    assert r["fp32_iterations"] == r["iterations"] > 0
+    k = oracle.rel_kkt(inst, r["x"], r["y"])
+    assert max(k["rel_primal"], k["rel_dual"], k["rel_gap"]) <= KKT_TOL, k
+    assert max(r["rel_primal"], r["rel_dual"], r["rel_gap"]) <= 1e-6
+    assert abs(r["objective"] - (-8206.12353127857)) <= 1e-6 * 8207

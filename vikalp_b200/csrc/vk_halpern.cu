@@ -582,7 +582,7 @@ public:
         c.limit = o_.iteration_limit;
         c.status = VK_STATUS_NOT_SOLVED;
         c.kkt = std::numeric_limits<double>::infinity();
-        VK_CUDA(cudaMemcpyAsync(ctl_.get(), &c, sizeof(c), cudaMemcpyHostToDevice, s_));
+        put_control(c);
     }
 
     // Times every FAST kernel variant on the two fused iteration passes of
@@ -678,7 +678,7 @@ public:
                     h.done = 0;
                     h.status = VK_STATUS_NOT_SOLVED;
                     h.tol = target;
-                    VK_CUDA(cudaMemcpyAsync(ctl_.get(), &h, sizeof(h), cudaMemcpyHostToDevice, s_));
+                    put_control(h);
                     continue;
                 }
                 best = std::min(best, h.kkt);
@@ -706,14 +706,14 @@ public:
                 h.rel_p = k64_.rel_p;
                 h.rel_d = k64_.rel_d;
                 h.rel_gap = k64_.rel_gap;
-                VK_CUDA(cudaMemcpyAsync(ctl_.get(), &h, sizeof(h), cudaMemcpyHostToDevice, s_));
+                put_control(h);
             } else if (h.status == VK_STATUS_OPTIMAL || h.status == VK_STATUS_NOT_SOLVED ||
                        h.status == VK_STATUS_ITERATION_LIMIT) {
                 h.done = 0;
                 h.status = VK_STATUS_NOT_SOLVED;
                 h.tol = o_.relative_tolerance;
                 h.limit = o_.iteration_limit + std::max<long long>(chunk_, 0); // the polish gets at least one check
-                VK_CUDA(cudaMemcpyAsync(ctl_.get(), &h, sizeof(h), cudaMemcpyHostToDevice, s_));
+                put_control(h);
             }
         }
         if (!timed_out && !confirmed) {
@@ -755,6 +755,13 @@ public:
     void set_limits(const vk_options &o) override { o_ = o; }
 
 private:
+    // Writes a control block to the device from the pinned host copy (later
+    // reads of it on the stream, poll_chunk's included, are ordered after).
+    void put_control(const HalCtl &h) {
+        hctl_[0] = h;
+        VK_CUDA(cudaMemcpyAsync(ctl_.get(), hctl_.get(), sizeof(HalCtl), cudaMemcpyHostToDevice, s_));
+    }
+
     // Relative KKT error, in float64, of the float32 state's last (x^, y^):
     // converted to float64, then the two float64 KKT passes and one
     // evaluation kernel -- no iteration. Leaves the float64 x^, y^ in place.
