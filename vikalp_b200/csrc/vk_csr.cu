@@ -4,7 +4,10 @@
 #include "vk_stage.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
+#include <cstring>
+#include <stdexcept>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
@@ -64,6 +67,19 @@ __global__ void gather_rows_kernel(const int *__restrict__ perm, const int *__re
                                    int *__restrict__ out) {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nnz; t += (int64_t)gridDim.x * blockDim.x)
         out[t] = rowidx[perm[t]];
+}
+
+// ci[k] = rank[ci[k]] (column renaming, in place)
+__global__ void rename_cols_kernel(int *__restrict__ ci, const int *__restrict__ rank, int64_t nnz) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nnz; t += (int64_t)gridDim.x * blockDim.x)
+        ci[t] = rank[ci[t]];
+}
+
+// dst[perm[t]] = src[t]
+__global__ void scatter_values_kernel(const int *__restrict__ perm, const double *__restrict__ src,
+                                      double *__restrict__ dst, int64_t n) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        dst[perm[t]] = src[t];
 }
 
 __global__ void tile_k_kernel(const int *__restrict__ ro, const int *__restrict__ tiles, int count,
@@ -263,6 +279,75 @@ void transpose_pattern(const CsrPattern32 &a, CsrPattern32 &at, DevBuf<int> &per
         at.max_row = mr;
     }
     build_tiles(at, s);
+}
+
+ColumnOrder column_order_mode() {
+    const char *e = std::getenv("VIKALP_B200_COLUMN_ORDER");
+    if (!e || !*e || std::strcmp(e, "auto") == 0) return ColumnOrder::Auto;
+    if (std::strcmp(e, "keep") == 0) return ColumnOrder::Keep;
+    if (std::strcmp(e, "count") == 0) return ColumnOrder::Count;
+    throw InvalidInput("VIKALP_B200_COLUMN_ORDER must be auto, keep or count");
+}
+
+bool order_columns_by_count(CsrPattern32 &a, ColumnOrder mode, DevBuf<int> &new_to_old, std::vector<int> &h_new_to_old,
+                            cudaStream_t s) {
+    h_new_to_old.clear();
+    const int n = a.cols;
+    const int64_t nnz = a.nnz;
+    if (mode == ColumnOrder::Keep || n <= 1 || nnz <= 0) return false;
+    if (mode == ColumnOrder::Auto && nnz < kOrderMinNnz) return false;
+    // nonzeros per column
+    std::vector<int> cnt(static_cast<size_t>(n) + 1);
+    {
+        DevBuf<int> dcnt(static_cast<size_t>(n) + 1);
+        VK_CUDA(cudaMemsetAsync(dcnt.get(), 0, dcnt.bytes(), s));
+        count_cols_kernel<<<grid_for(nnz), 256, 0, s>>>(a.ci.get(), nnz, dcnt.get());
+        VK_LAUNCH_CHECK();
+        VK_CUDA(cudaMemcpyAsync(cnt.data(), dcnt.get(), cnt.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+        VK_CUDA(cudaStreamSynchronize(s));
+    }
+    const int *c = cnt.data() + 1;
+    int most = 0;
+    double var = 0.0;
+    const double mean = static_cast<double>(nnz) / n;
+    for (int j = 0; j < n; ++j) {
+        most = std::max(most, c[j]);
+        var += (c[j] - mean) * (c[j] - mean);
+    }
+    const double cv = std::sqrt(var / n) / mean;
+    if (mode == ColumnOrder::Auto && cv < kOrderMinSpread) return false;
+    // stable counting sort, most nonzeros first: start[v] = columns with more than v nonzeros
+    std::vector<int64_t> start(static_cast<size_t>(most) + 2, 0);
+    for (int j = 0; j < n; ++j) ++start[c[j]];
+    int64_t above = 0;
+    for (int v = most; v >= 0; --v) {
+        const int64_t k = start[v];
+        start[v] = above;
+        above += k;
+    }
+    std::vector<int> rank(static_cast<size_t>(n));
+    h_new_to_old.assign(static_cast<size_t>(n), 0);
+    for (int j = 0; j < n; ++j) {
+        const int r = static_cast<int>(start[c[j]]++);
+        rank[j] = r;
+        h_new_to_old[r] = j;
+    }
+    DevBuf<int> drank(static_cast<size_t>(n));
+    new_to_old.reset(static_cast<size_t>(n));
+    VK_CUDA(cudaMemcpyAsync(drank.get(), rank.data(), rank.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    VK_CUDA(cudaMemcpyAsync(new_to_old.get(), h_new_to_old.data(), h_new_to_old.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, s));
+    rename_cols_kernel<<<grid_for(nnz), 256, 0, s>>>(a.ci.get(), drank.get(), nnz);
+    VK_LAUNCH_CHECK();
+    VK_CUDA(cudaStreamSynchronize(s)); // drank and the host vectors go out of scope
+    a.fp = mix_fingerprint(a.fp, 0x636f6c636f756e74ull); // "colcount"
+    return true;
+}
+
+void scatter_values(const int *perm, const double *src, double *dst, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    scatter_values_kernel<<<grid_for(n), 256, 0, s>>>(perm, src, dst, n);
+    VK_LAUNCH_CHECK();
 }
 
 template <class TD, class TS>

@@ -45,6 +45,7 @@
 #include "vk_common.cuh"
 
 #include <algorithm>
+#include <vector>
 
 namespace vk {
 
@@ -1108,6 +1109,26 @@ void build_tiles(CsrPattern32 &p, cudaStream_t s, const unsigned char *breaks = 
 // Transposes `a` on the device by a stable radix sort of the column indices
 // (rows ascend within each column). perm[t] = source position of entry t.
 void transpose_pattern(const CsrPattern32 &a, CsrPattern32 &at, DevBuf<int> &perm, cudaStream_t s);
+
+// Column order of the FAST passes (VIKALP_B200_COLUMN_ORDER = auto | keep |
+// count): `count` renames a pattern's columns in order of decreasing
+// nonzero count, ties in their original order; `auto` does so when the
+// pattern has at least kOrderMinNnz nonzeros and the counts' coefficient of
+// variation is at least kOrderMinSpread (skewed, power-law columns). The
+// transpose's rows then come longest first, which evens the work of the
+// warps of the transposed pass, and the most gathered entries of x sit
+// together. Parity modes keep the order.
+enum class ColumnOrder { Auto, Keep, Count };
+constexpr int64_t kOrderMinNnz = int64_t(1) << 20;
+constexpr double kOrderMinSpread = 1.0;
+ColumnOrder column_order_mode(); // throws InvalidInput on a bad value
+// Renames a's columns (a.ci, a.fp) when `mode` asks for it; new_to_old[j'] is
+// the original column of new column j' (device and host copies). Returns
+// false, leaving everything untouched, when the order is kept.
+bool order_columns_by_count(CsrPattern32 &a, ColumnOrder mode, DevBuf<int> &new_to_old, std::vector<int> &h_new_to_old,
+                            cudaStream_t s);
+// dst[perm[t]] = src[t], t < n
+void scatter_values(const int *perm, const double *src, double *dst, int64_t n, cudaStream_t s);
 // dst[t] = src[perm[t]] (optionally converting the value type).
 template <class TD, class TS>
 void gather_values(const int *perm, const TS *src, TD *dst, int64_t nnz, cudaStream_t s);

@@ -163,10 +163,13 @@ __global__ void scal_kernel(T *__restrict__ a, int n, const double *__restrict__
     if (i < n) a[i] = static_cast<T>(a[i] * s);
 }
 
-__global__ void seed_kernel(double *a, int n) {
+// the power iteration's start vector, a hash of each column's index in the
+// caller's order (perm: device column -> caller's column, or nullptr), so a
+// renamed model starts from the same vector
+__global__ void seed_kernel(double *a, int n, const int *__restrict__ perm) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
-        unsigned h = static_cast<unsigned>(i) * 2654435761u + 12345u;
+        unsigned h = static_cast<unsigned>(perm ? perm[i] : i) * 2654435761u + 12345u;
         h ^= h >> 13;
         h *= 2246822519u;
         h ^= h >> 16;
@@ -867,7 +870,7 @@ private:
     void step_size() {
         const int m = dm_.m, n = dm_.n;
         DevBuf<double> v(n), w(m > 0 ? m : 1), z(n), part(1024), nrm(1);
-        seed_kernel<<<grid1d(n), 256, 0, s_>>>(v.get(), n);
+        seed_kernel<<<grid1d(n), 256, 0, s_>>>(v.get(), n, dm_.reordered() ? dm_.cperm.get() : nullptr);
         VK_LAUNCH_CHECK();
         auto norm2 = [&](const double *a, int k) {
             dot_kernel<double><<<std::min(1024, grid1d(k)), 256, 0, s_>>>(a, a, k, part.get());
@@ -905,7 +908,7 @@ private:
         // lambda_max(Q^) by power iteration on Q^ (PSD), same start and stopping rule
         lq_ = 0.0;
         if (dm_.qp && dm_.q_nnz > 0) {
-            seed_kernel<<<grid1d(n), 256, 0, s_>>>(v.get(), n);
+            seed_kernel<<<grid1d(n), 256, 0, s_>>>(v.get(), n, dm_.reordered() ? dm_.cperm.get() : nullptr);
             norm2(v.get(), n);
             scal_kernel<double><<<grid1d(n), 256, 0, s_>>>(v.get(), n, nrm.get());
             double prev = 0.0;
@@ -939,8 +942,8 @@ private:
         VK_CUDA(cudaStreamSynchronize(s_));
         double c2 = 0.0, cs2 = 0.0, b2 = 0.0, bs2 = 0.0;
         for (int j = 0; j < n; ++j) {
-            c2 += dm_.h_c[j] * dm_.h_c[j];
-            const double t = dm_.h_c[j] * hcs[j];
+            c2 += dm_.c_dev(j) * dm_.c_dev(j);
+            const double t = dm_.c_dev(j) * hcs[j];
             cs2 += t * t;
         }
         for (int i = 0; i < m; ++i) {

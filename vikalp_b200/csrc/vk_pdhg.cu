@@ -236,7 +236,7 @@ void ensure_tuned(DeviceModel &dm, cudaStream_t s) {
     dm.tuned = true;
 }
 
-std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s, int verbose) {
+std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s, int verbose, bool reorder) {
     PhaseLog log(verbose, "upload", s);
     auto dm = std::make_unique<DeviceModel>();
     const int64_t m = p.A.rows, n = p.A.cols;
@@ -249,6 +249,8 @@ std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s, i
     static const int64_t zero = 0;
     upload_pattern(m, n, m > 0 ? p.A.row_offsets : &zero, p.A.col_indices, dm->a, s);
     log.mark("pattern (int64 -> int32) + tiles");
+    if (reorder && !dm->qp && order_columns_by_count(dm->a, column_order_mode(), dm->cperm, dm->h_cperm, s))
+        log.mark("column order (by nonzero count)");
     dm->a_val.reset(padded(dm->nnz));
     stage_h2d(dm->a_val.get(), p.A.values, dm->nnz * sizeof(double), s);
     log.mark("values");
@@ -268,9 +270,18 @@ std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s, i
         b.reset(k > 0 ? k : 1);
         if (k > 0) stage_h2d(b.get(), h, k * sizeof(double), s);
     };
-    up(dm->c, p.c, n);
-    up(dm->vl, p.var_lower, n);
-    up(dm->vu, p.var_upper, n);
+    // column vectors into the device's column order
+    auto upcol = [&](DevBuf<double> &b, const double *h) {
+        if (!dm->reordered()) return up(b, h, n);
+        DevBuf<double> t;
+        up(t, h, n);
+        b.reset(n);
+        gather_values<double, double>(dm->cperm.get(), t.get(), b.get(), n, s);
+        VK_CUDA(cudaStreamSynchronize(s)); // t goes out of scope
+    };
+    upcol(dm->c, p.c);
+    upcol(dm->vl, p.var_lower);
+    upcol(dm->vu, p.var_upper);
     up(dm->rl, p.row_lower, m);
     up(dm->ru, p.row_upper, m);
     dm->h_c.assign(p.c, p.c + n);
@@ -449,7 +460,7 @@ Solver::Solver(const vk_problem &p, const vk_options &o) : opts_(o) {
     device_error_flag(); // allocated here, never inside a graph capture
     VK_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     PhaseLog log(o.verbose, "create", stream_);
-    dm_ = upload_model(p, stream_, o.verbose);
+    dm_ = upload_model(p, stream_, o.verbose, o.spmv_order == VK_SPMV_FAST);
     log.mark("upload + transpose");
     // the Halpern passes (and the reference scheme's Q pass) run on the
     // patterns' tuned variants; the reference scheme tunes its fused passes itself
@@ -499,10 +510,12 @@ Solver::~Solver() {
 }
 
 namespace {
-__global__ void fill_override_kernel(const double *__restrict__ ov, const double *__restrict__ model, int n,
-                                     double *__restrict__ out) {
+// out[j] = the override of device column j (the caller's column perm[j], or
+// j without a column order), else the model's bound
+__global__ void fill_override_kernel(const double *__restrict__ ov, const double *__restrict__ model,
+                                     const int *__restrict__ perm, int n, double *__restrict__ out) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j < n) out[j] = ov ? ov[j] : model[j];
+    if (j < n) out[j] = ov ? ov[perm ? perm[j] : j] : model[j];
 }
 } // namespace
 
@@ -542,15 +555,19 @@ void Solver::solve(const double *warm, const double *lo_ovr, const double *hi_ov
     if (lo_ovr) VK_CUDA(cudaMemcpyAsync(ov_lo.get(), lo_ovr, n * sizeof(double), cudaMemcpyHostToDevice, s));
     if (hi_ovr) VK_CUDA(cudaMemcpyAsync(ov_hi.get(), hi_ovr, n * sizeof(double), cudaMemcpyHostToDevice, s));
     if (warm) VK_CUDA(cudaMemcpyAsync(dwarm.get(), warm, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    fill_override_kernel<<<grid1d(n), 256, 0, s>>>(lo_ovr ? ov_lo.get() : nullptr, dm.vl.get(), n, lo.get());
-    fill_override_kernel<<<grid1d(n), 256, 0, s>>>(hi_ovr ? ov_hi.get() : nullptr, dm.vu.get(), n, hi.get());
+    const int *cperm = dm.reordered() ? dm.cperm.get() : nullptr;
+    fill_override_kernel<<<grid1d(n), 256, 0, s>>>(lo_ovr ? ov_lo.get() : nullptr, dm.vl.get(), cperm, n, lo.get());
+    fill_override_kernel<<<grid1d(n), 256, 0, s>>>(hi_ovr ? ov_hi.get() : nullptr, dm.vu.get(), cperm, n, hi.get());
     VK_LAUNCH_CHECK();
+    DevBuf<double> dwarm_dev(warm && cperm ? n : 0); // the warm start in the device's column order
+    if (warm && cperm) gather_values<double, double>(cperm, dwarm.get(), dwarm_dev.get(), n, s);
+    const double *warm_dev = !warm ? nullptr : cperm ? dwarm_dev.get() : dwarm.get();
 
     DevBuf<double> xo(n), yo(m > 0 ? m : 1);
     RunInfo info;
     PhaseLog log(opts_.verbose, "solve", s);
     log.mark("checks + overrides");
-    engine_->run(warm ? dwarm.get() : nullptr, lo.get(), hi.get(), xo.get(), yo.get(), info, started);
+    engine_->run(warm_dev, lo.get(), hi.get(), xo.get(), yo.get(), info, started);
     log.mark("iterations");
 
     // post-processing
@@ -609,13 +626,28 @@ void Solver::solve(const double *warm, const double *lo_ovr, const double *hi_ov
     double hs[kPostRowSums + kPostColSums];
     VK_CUDA(cudaMemcpyAsync(&hp, post.get(), sizeof(hp), cudaMemcpyDeviceToHost, s));
     VK_CUDA(cudaMemcpyAsync(hs, sums.get(), sizeof(hs), cudaMemcpyDeviceToHost, s));
+    // column-indexed results back into the caller's column order
+    DevBuf<double> back(cperm ? 3 * static_cast<size_t>(n) : 0);
+    const double *x_out = xo.get(), *vld_out = vld.get(), *vud_out = vud.get();
+    if (cperm) {
+        scatter_values(cperm, xo.get(), back.get(), n, s);
+        x_out = back.get();
+        if (r->var_lower_dual) {
+            scatter_values(cperm, vld.get(), back.get() + n, n, s);
+            vld_out = back.get() + n;
+        }
+        if (r->var_upper_dual) {
+            scatter_values(cperm, vud.get(), back.get() + 2 * static_cast<size_t>(n), n, s);
+            vud_out = back.get() + 2 * static_cast<size_t>(n);
+        }
+    }
     std::vector<double> hx(n);
-    stage_d2h(hx.data(), xo.get(), n * sizeof(double), s);
+    stage_d2h(hx.data(), x_out, n * sizeof(double), s);
     if (r->y && m > 0) stage_d2h(r->y, yo.get(), m * sizeof(double), s);
     if (r->row_lower_dual && m > 0) stage_d2h(r->row_lower_dual, ld.get(), m * sizeof(double), s);
     if (r->row_upper_dual && m > 0) stage_d2h(r->row_upper_dual, ud.get(), m * sizeof(double), s);
-    if (r->var_lower_dual) stage_d2h(r->var_lower_dual, vld.get(), n * sizeof(double), s);
-    if (r->var_upper_dual) stage_d2h(r->var_upper_dual, vud.get(), n * sizeof(double), s);
+    if (r->var_lower_dual) stage_d2h(r->var_lower_dual, vld_out, n * sizeof(double), s);
+    if (r->var_upper_dual) stage_d2h(r->var_upper_dual, vud_out, n * sizeof(double), s);
     VK_CUDA(cudaStreamSynchronize(s));
     if (r->x) std::memcpy(r->x, hx.data(), n * sizeof(double));
 

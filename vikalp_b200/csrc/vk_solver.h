@@ -26,6 +26,15 @@ struct DeviceModel {
     std::vector<double> h_qv;
     std::vector<double> h_vl, h_vu;          // model bounds (override validation)
     bool tuned = false;                      // pattern variants timed (ensure_tuned)
+    // Column order (order_columns_by_count): when cperm is set, the device
+    // side (a, at, a_val, at_val, c, vl, vu) is in the renamed order and
+    // column j' holds original column cperm[j']; the host copies above stay
+    // in the caller's order.
+    DevBuf<int> cperm;
+    std::vector<int> h_cperm;
+    bool reordered() const { return !h_cperm.empty(); }
+    // c of device column j'
+    double c_dev(int j) const { return h_c[reordered() ? h_cperm[j] : j]; }
 };
 
 // Device control block of the reference scheme (pdhg.cpp:75-150).
@@ -83,7 +92,9 @@ std::string validate_problem(const vk_problem &p, const vk_options &o, bool &uns
 // Uploads a validated problem. The sparse-pass variants of its patterns are
 // timed on first need (ensure_tuned): engines whose passes use the patterns'
 // variants call it; the reference scheme tunes its own two fused passes.
-std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s, int verbose = 0);
+// `reorder`: the column order may change (FAST passes); parity modes pass
+// false and keep the caller's order.
+std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s, int verbose = 0, bool reorder = false);
 void ensure_tuned(DeviceModel &dm, cudaStream_t s);
 
 // Independent LPs solved together (vk_batch.cu); throws on invalid input.
