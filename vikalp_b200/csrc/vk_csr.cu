@@ -75,6 +75,39 @@ __global__ void rename_cols_kernel(int *__restrict__ ci, const int *__restrict__
         ci[t] = rank[ci[t]];
 }
 
+// stats[0] = max cnt[j], stats[1] = sum of cnt[j]^2 (integers: exact, order-free)
+__global__ void count_stats_kernel(const int *__restrict__ cnt, int n, unsigned long long *__restrict__ stats) {
+    unsigned long long mx = 0, sq = 0;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const unsigned long long c = static_cast<unsigned long long>(cnt[j]);
+        mx = c > mx ? c : mx;
+        sq += c * c;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long m2 = __shfl_xor_sync(0xffffffffu, mx, o);
+        mx = m2 > mx ? m2 : mx;
+        sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(stats, mx);
+        atomicAdd(stats + 1, sq);
+    }
+}
+
+// keys[j] = most - cnt[j] (ascending keys: most nonzeros first), iota[j] = j
+__global__ void order_keys_kernel(const int *__restrict__ cnt, int n, int most, int *__restrict__ keys,
+                                  int *__restrict__ iota) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        keys[j] = most - cnt[j];
+        iota[j] = j;
+    }
+}
+
+// rank[new_to_old[i]] = i
+__global__ void invert_perm_kernel(const int *__restrict__ new_to_old, int n, int *__restrict__ rank) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) rank[new_to_old[i]] = i;
+}
+
 // dst[perm[t]] = src[t]
 __global__ void scatter_values_kernel(const int *__restrict__ perm, const double *__restrict__ src,
                                       double *__restrict__ dst, int64_t n) {
@@ -289,57 +322,43 @@ ColumnOrder column_order_mode() {
     throw InvalidInput("VIKALP_B200_COLUMN_ORDER must be auto, keep or count");
 }
 
-bool order_columns_by_count(CsrPattern32 &a, ColumnOrder mode, DevBuf<int> &new_to_old, std::vector<int> &h_new_to_old,
-                            cudaStream_t s) {
-    h_new_to_old.clear();
+bool order_columns_by_count(CsrPattern32 &a, ColumnOrder mode, DevBuf<int> &new_to_old, cudaStream_t s) {
     const int n = a.cols;
     const int64_t nnz = a.nnz;
     if (mode == ColumnOrder::Keep || n <= 1 || nnz <= 0) return false;
     if (mode == ColumnOrder::Auto && nnz < kOrderMinNnz) return false;
-    // nonzeros per column
-    std::vector<int> cnt(static_cast<size_t>(n) + 1);
-    {
-        DevBuf<int> dcnt(static_cast<size_t>(n) + 1);
-        VK_CUDA(cudaMemsetAsync(dcnt.get(), 0, dcnt.bytes(), s));
-        count_cols_kernel<<<grid_for(nnz), 256, 0, s>>>(a.ci.get(), nnz, dcnt.get());
-        VK_LAUNCH_CHECK();
-        VK_CUDA(cudaMemcpyAsync(cnt.data(), dcnt.get(), cnt.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
-        VK_CUDA(cudaStreamSynchronize(s));
-    }
-    const int *c = cnt.data() + 1;
-    int most = 0;
-    double var = 0.0;
-    const double mean = static_cast<double>(nnz) / n;
-    for (int j = 0; j < n; ++j) {
-        most = std::max(most, c[j]);
-        var += (c[j] - mean) * (c[j] - mean);
-    }
-    const double cv = std::sqrt(var / n) / mean;
-    if (mode == ColumnOrder::Auto && cv < kOrderMinSpread) return false;
-    // stable counting sort, most nonzeros first: start[v] = columns with more than v nonzeros
-    std::vector<int64_t> start(static_cast<size_t>(most) + 2, 0);
-    for (int j = 0; j < n; ++j) ++start[c[j]];
-    int64_t above = 0;
-    for (int v = most; v >= 0; --v) {
-        const int64_t k = start[v];
-        start[v] = above;
-        above += k;
-    }
-    std::vector<int> rank(static_cast<size_t>(n));
-    h_new_to_old.assign(static_cast<size_t>(n), 0);
-    for (int j = 0; j < n; ++j) {
-        const int r = static_cast<int>(start[c[j]]++);
-        rank[j] = r;
-        h_new_to_old[r] = j;
-    }
-    DevBuf<int> drank(static_cast<size_t>(n));
-    new_to_old.reset(static_cast<size_t>(n));
-    VK_CUDA(cudaMemcpyAsync(drank.get(), rank.data(), rank.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-    VK_CUDA(cudaMemcpyAsync(new_to_old.get(), h_new_to_old.data(), h_new_to_old.size() * sizeof(int),
-                            cudaMemcpyHostToDevice, s));
-    rename_cols_kernel<<<grid_for(nnz), 256, 0, s>>>(a.ci.get(), drank.get(), nnz);
+    // nonzeros per column (cnt[j + 1]) and their largest value and sum of squares
+    DevBuf<int> cnt(static_cast<size_t>(n) + 1);
+    DevBuf<unsigned long long> stats(2);
+    VK_CUDA(cudaMemsetAsync(cnt.get(), 0, cnt.bytes(), s));
+    VK_CUDA(cudaMemsetAsync(stats.get(), 0, stats.bytes(), s));
+    count_cols_kernel<<<grid_for(nnz), 256, 0, s>>>(a.ci.get(), nnz, cnt.get());
+    count_stats_kernel<<<grid_for(n), 256, 0, s>>>(cnt.get() + 1, n, stats.get());
     VK_LAUNCH_CHECK();
-    VK_CUDA(cudaStreamSynchronize(s)); // drank and the host vectors go out of scope
+    unsigned long long h[2] = {0, 0};
+    VK_CUDA(cudaMemcpyAsync(h, stats.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    VK_CUDA(cudaStreamSynchronize(s));
+    const int most = static_cast<int>(h[0]);
+    const double mean = static_cast<double>(nnz) / n;
+    const double var = std::max(0.0, static_cast<double>(h[1]) / n - mean * mean);
+    if (mode == ColumnOrder::Auto && std::sqrt(var) < kOrderMinSpread * mean) return false;
+    // stable sort on (most - count): most nonzeros first, ties in the caller's order
+    DevBuf<int> keys(static_cast<size_t>(n)), keys_out(static_cast<size_t>(n)), iota(static_cast<size_t>(n)),
+        rank(static_cast<size_t>(n));
+    new_to_old.reset(static_cast<size_t>(n));
+    order_keys_kernel<<<grid_for(n), 256, 0, s>>>(cnt.get() + 1, n, most, keys.get(), iota.get());
+    VK_LAUNCH_CHECK();
+    size_t tb = 0;
+    const int end_bit = bits_for(most);
+    VK_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.get(), keys_out.get(), iota.get(), new_to_old.get(), n, 0,
+                                            end_bit, s));
+    DevBuf<unsigned char> tmp(tb > 0 ? tb : 1);
+    VK_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, keys.get(), keys_out.get(), iota.get(), new_to_old.get(), n,
+                                            0, end_bit, s));
+    invert_perm_kernel<<<grid_for(n), 256, 0, s>>>(new_to_old.get(), n, rank.get());
+    rename_cols_kernel<<<grid_for(nnz), 256, 0, s>>>(a.ci.get(), rank.get(), nnz);
+    VK_LAUNCH_CHECK();
+    VK_CUDA(cudaStreamSynchronize(s)); // the temporaries go out of scope
     a.fp = mix_fingerprint(a.fp, 0x636f6c636f756e74ull); // "colcount"
     return true;
 }

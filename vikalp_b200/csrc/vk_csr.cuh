@@ -1122,11 +1122,11 @@ enum class ColumnOrder { Auto, Keep, Count };
 constexpr int64_t kOrderMinNnz = int64_t(1) << 20;
 constexpr double kOrderMinSpread = 1.0;
 ColumnOrder column_order_mode(); // throws InvalidInput on a bad value
-// Renames a's columns (a.ci, a.fp) when `mode` asks for it; new_to_old[j'] is
-// the original column of new column j' (device and host copies). Returns
-// false, leaving everything untouched, when the order is kept.
-bool order_columns_by_count(CsrPattern32 &a, ColumnOrder mode, DevBuf<int> &new_to_old, std::vector<int> &h_new_to_old,
-                            cudaStream_t s);
+// Renames a's columns (a.ci, a.fp) when `mode` asks for it, all on the
+// device (a stable radix sort of the counts); new_to_old[j'] is the original
+// column of new column j'. Returns false, leaving everything untouched, when
+// the order is kept.
+bool order_columns_by_count(CsrPattern32 &a, ColumnOrder mode, DevBuf<int> &new_to_old, cudaStream_t s);
 // dst[perm[t]] = src[t], t < n
 void scatter_values(const int *perm, const double *src, double *dst, int64_t n, cudaStream_t s);
 // dst[t] = src[perm[t]] (optionally converting the value type).

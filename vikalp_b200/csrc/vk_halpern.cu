@@ -934,6 +934,7 @@ private:
         // |c^| and |b^| (scaled) for omega_0; |c| and |b| original for the KKT scales
         std::vector<double> hc(n), hrl(m), hru(m), hcs(n), hrs(m);
         VK_CUDA(cudaMemcpyAsync(hcs.data(), cs_.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s_));
+        VK_CUDA(cudaMemcpyAsync(hc.data(), dm_.c.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s_)); // device order
         if (m > 0) {
             VK_CUDA(cudaMemcpyAsync(hrs.data(), rs_.get(), m * sizeof(double), cudaMemcpyDeviceToHost, s_));
             VK_CUDA(cudaMemcpyAsync(hrl.data(), dm_.rl.get(), m * sizeof(double), cudaMemcpyDeviceToHost, s_));
@@ -942,8 +943,8 @@ private:
         VK_CUDA(cudaStreamSynchronize(s_));
         double c2 = 0.0, cs2 = 0.0, b2 = 0.0, bs2 = 0.0;
         for (int j = 0; j < n; ++j) {
-            c2 += dm_.c_dev(j) * dm_.c_dev(j);
-            const double t = dm_.c_dev(j) * hcs[j];
+            c2 += hc[j] * hc[j];
+            const double t = hc[j] * hcs[j];
             cs2 += t * t;
         }
         for (int i = 0; i < m; ++i) {

@@ -249,7 +249,7 @@ std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s, i
     static const int64_t zero = 0;
     upload_pattern(m, n, m > 0 ? p.A.row_offsets : &zero, p.A.col_indices, dm->a, s);
     log.mark("pattern (int64 -> int32) + tiles");
-    if (reorder && !dm->qp && order_columns_by_count(dm->a, column_order_mode(), dm->cperm, dm->h_cperm, s))
+    if (reorder && !dm->qp && order_columns_by_count(dm->a, column_order_mode(), dm->cperm, s))
         log.mark("column order (by nonzero count)");
     dm->a_val.reset(padded(dm->nnz));
     stage_h2d(dm->a_val.get(), p.A.values, dm->nnz * sizeof(double), s);
@@ -270,14 +270,16 @@ std::unique_ptr<DeviceModel> upload_model(const vk_problem &p, cudaStream_t s, i
         b.reset(k > 0 ? k : 1);
         if (k > 0) stage_h2d(b.get(), h, k * sizeof(double), s);
     };
-    // column vectors into the device's column order
+    // column vectors into the device's column order (the caller's order lands
+    // in `orig`, kept until the stream synchronises below)
+    DevBuf<double> orig[3];
+    int used = 0;
     auto upcol = [&](DevBuf<double> &b, const double *h) {
         if (!dm->reordered()) return up(b, h, n);
-        DevBuf<double> t;
-        up(t, h, n);
+        up(orig[used], h, n);
         b.reset(n);
-        gather_values<double, double>(dm->cperm.get(), t.get(), b.get(), n, s);
-        VK_CUDA(cudaStreamSynchronize(s)); // t goes out of scope
+        gather_values<double, double>(dm->cperm.get(), orig[used].get(), b.get(), n, s);
+        ++used;
     };
     upcol(dm->c, p.c);
     upcol(dm->vl, p.var_lower);

@@ -31,10 +31,7 @@ struct DeviceModel {
     // column j' holds original column cperm[j']; the host copies above stay
     // in the caller's order.
     DevBuf<int> cperm;
-    std::vector<int> h_cperm;
-    bool reordered() const { return !h_cperm.empty(); }
-    // c of device column j'
-    double c_dev(int j) const { return h_c[reordered() ? h_cperm[j] : j]; }
+    bool reordered() const { return cperm.get() != nullptr; }
 };
 
 // Device control block of the reference scheme (pdhg.cpp:75-150).
