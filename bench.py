@@ -475,11 +475,12 @@ def main():
     prof = h.profile(2 * CHUNK) if rank == 0 else None
     h.close()
     # ---- e2e: through the C ABI from host arrays ---------------------------------
-    # five calls (each: create with upload and device setup, solve, results
+    # nine calls (each: create with upload and device setup, solve, results
     # back); the median is reported: the host side (page faults of fresh
-    # result arrays, driver allocations) varies from call to call
+    # result arrays, driver allocations, a shared host's other work) varies
+    # from call to call, by up to ~0.7 s on some boxes
     runs, creates = [], []
-    for _ in range(5):
+    for _ in range(9):
         replicas.barrier(ranks)
         t0 = time.perf_counter()
         with vk.Pdhg(inst, algorithm="reference", iteration_limit=K * CHUNK, primal_tolerance=0.0,
@@ -497,7 +498,7 @@ def main():
            "h2d_bytes_per_step": int(h2d / steps_e2e), "d2h_bytes_per_step": int(d2h / steps_e2e),
            "seconds": round(t_e2e, 3), "runs_seconds": [round(t, 3) for _, t in runs],
            "create_seconds": [round(t, 3) for t in creates],
-           "note": "create (upload + device setup) + solve + results, pageable host arrays; median of 5 calls"}
+           "note": "create (upload + device setup) + solve + results, pageable host arrays; median of 9 calls"}
     line = {"metric": METRIC, "value": round(value, 3), "unit": "iter/s", "n_gpus": ws, "steps": iters // CHUNK,
             "warmup": W, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,

@@ -1171,8 +1171,9 @@ int tuned_pick(uint64_t key, F &&tune) {
     return store_pick(key, tune());
 }
 
-// Fingerprint of a host CSR pattern (rows, cols, every row offset, every
-// 61st column index and the last one), FNV-1a over 64-bit words.
+// Fingerprint of a host CSR pattern (rows, cols, every 61st row offset and
+// column index and the last of each), FNV-1a over 64-bit words; it keys the
+// kernel-pick cache only.
 uint64_t pattern_fingerprint(int64_t rows, int64_t cols, const int64_t *ro, const int64_t *ci);
 uint64_t mix_fingerprint(uint64_t a, uint64_t b);
 

@@ -191,7 +191,7 @@ void stage_h2d_narrow(int *dst, const int64_t *src, int64_t count, cudaStream_t 
         pending = true;
         VK_CUDA(cudaMemcpyAsync(dst + b, buf, n * sizeof(int), cudaMemcpyHostToDevice, s));
         VK_CUDA(cudaEventRecord(ev, s));
-    });
+    }, kStageThreadsNarrow);
 }
 
 void stage_d2h(void *dst, const void *src, size_t bytes, cudaStream_t s) {

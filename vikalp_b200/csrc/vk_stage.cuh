@@ -27,6 +27,9 @@ constexpr int kStageThreads = 4;
 // different pages in parallel, so downloads spread over more threads. Their
 // extra pinned buffers join the process-wide pool on first use.
 constexpr int kStageThreadsD2H = 16;
+// int64 -> int32 uploads convert on the host threads (the CSR's indices), which
+// bounds them by the threads' loads and stores, not by the DMA: more threads.
+constexpr int kStageThreadsNarrow = 8;
 
 // dst (device) <- src (host), `bytes` bytes.
 void stage_h2d(void *dst, const void *src, size_t bytes, cudaStream_t s);
