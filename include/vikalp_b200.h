@@ -137,7 +137,11 @@ const char *vk_version(void);
  * (Model.cpp:118-199, continuous_common.hpp:80-126), copies it to the GPU and
  * builds every device-side structure (int32 CSR, transposed CSR, scaling,
  * tile schedules). Replaces the setup half of solve_scaled_lp / qp
- * (pdhg.cpp:20-80, pdqp.cpp:20-103). */
+ * (pdhg.cpp:20-80, pdqp.cpp:20-103). With VK_SPMV_FAST an LP whose column
+ * nonzero counts are skewed gets its columns renamed internally in order of
+ * decreasing count (environment VIKALP_B200_COLUMN_ORDER = auto | keep |
+ * count, read here; any other value fails with VK_ERR_INVALID); overrides,
+ * warm starts and results stay in the caller's column order. */
 int vk_pdhg_create(const vk_problem *problem, const vk_options *opts, vk_pdhg **out);
 
 /* Runs the solve. warm_start, var_lower_override and var_upper_override are
